@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark: coupled 1 ms epochs/s of the full-resolution coupled laser-tissue run.
+
+Workload (seeded synthetic, no dataset): 200x200x128 layered beetle stack + 64 air slices for the
+plume (200x200x192 voxels at 15 um), 532 nm, 40 W Gaussian 0.5 mm spot at 22 deg, 150k photons per
+laser epoch, 20 x 50 us substeps, boiling / char / ablation / plume (D, extinction, char kinetics
+drawn from the seed). A step is one 1 ms epoch; the laser is on for the first 20 % of the timed
+epochs (the 200-on / 800-off duty of the 1000-epoch production schedule) and off after.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: replicas only (independent instances, one per rank; no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "coupled 1 ms epochs/s (full-resolution coupled run)"
+FALLBACK_HBM_GBS = 6650.0
+LASER_DUTY = 0.2
+POWER_W = 40.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--small", action="store_true", help="64x64x128 grid (profiling / smoke only, not a bench line)")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", FALLBACK_HBM_GBS)), "measured", d
+    return FALLBACK_HBM_GBS, "fallback", {}
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        for line in Path(self.f.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(float(r[2]) for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def cpu_port_baseline(geo, kw, on_epochs=1, off_epochs=1, warm=True):
+    """Time the oracle port (FP64 C kernels of the reference CPU path) on a bounded sample:
+    laser-on and laser-off epochs of the same workload; full-run epochs/s = 1000 / (200 t_on + 800 t_off)."""
+    import oracle
+    from oracle.engine import OracleEngine
+    oracle.build()
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    eng = OracleEngine(**kw, plume_dt_policy="subcycle")
+    t_on, t_off = [], []
+    for i in range(on_epochs):
+        eng.power = POWER_W
+        t0 = time.perf_counter(); eng.step_epoch(); t_on.append(time.perf_counter() - t0)
+    for i in range(off_epochs):
+        eng.power = 0.0
+        t0 = time.perf_counter(); eng.step_epoch(); t_off.append(time.perf_counter() - t0)
+    ton, toff = statistics.median(t_on), statistics.median(t_off)
+    per_epoch = LASER_DUTY * ton + (1 - LASER_DUTY) * toff
+    return {"value": 1.0 / per_epoch, "unit": "epochs/s", "cores": threads, "kind": "port",
+            "sample": f"{on_epochs} laser-on + {off_epochs} laser-off epoch(s) of the same workload on the FP64 C port "
+                      f"of the reference CPU path (oracle/orc.c, OpenMP); t_on={ton:.3f}s t_off={toff:.3f}s; "
+                      f"value = 1/(0.2 t_on + 0.8 t_off)",
+            "t_on_s": ton, "t_off_s": toff}
+
+
+def make_engine(geo, dev, seed_offset=0):
+    from bug_defense_b200 import CoupledAblationEngine
+    from bug_defense_b200.workloads import engine_kwargs
+    kw = engine_kwargs(geo)
+    kw["seed"] = kw["seed"] + seed_offset
+    return CoupledAblationEngine(**kw, device=dev)
+
+
+def algorithmic_bytes(geo, eng):
+    """Unique bytes each stage must move per launch (cache-ideal neighbours)."""
+    nv = eng.Nx * eng.Ny * eng.Nz
+    # fused substep: T r+w 8, k 4, rho 4, source 4, flags 1, H r+w 8, chi r+w 8
+    sub = nv * 37
+    # plume step: C r+w 8, flags 1
+    plume = nv * 9
+    return {"substep": sub, "plume_step": plume}
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    from bug_defense_b200 import _lib, workloads
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    geo = workloads.full_coupled_run(seed=args.seed) if not args.small else workloads.full_coupled_run(
+        seed=args.seed, nx=64, ny=64)
+    eng = make_engine(geo, dev, seed_offset=rank)
+    K, W = int(args.steps), int(args.warmup)
+    n_on = max(1, int(round(LASER_DUTY * K)))
+    for _ in range(W):
+        eng.power = POWER_W
+        eng._enqueue(0)
+    torch.cuda.synchronize()
+    lib = _lib.load()
+    lib.bd_engine_timing(eng._handle, 1)
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(st)
+        for s in range(K):
+            eng.power = POWER_W if s < n_on else 0.0
+            eng._enqueue(0)
+        e1.record(st)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    stage = (ctypes.c_double * 4)()
+    nep = ctypes.c_int64(0)
+    _lib.check(lib.bd_engine_timing_read(eng._handle, stage, ctypes.byref(nep)))
+    lib.bd_engine_timing(eng._handle, 0)
+    stage_ms = list(stage)
+    d = eng._diag(None)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    res = {"ms": ms, "K": K, "n_on": n_on, "stage_ms": stage_ms, "clocks": clk.summary(), "eng": eng, "geo": geo,
+           "last_diag": d}
+    return res
+
+
+def e2e_run(args, geo, dev, K):
+    """Same metric through the public API from host arrays: engine construction (upload of every
+    field from host numpy), K epochs each returning the diagnostics dict and pulling the runner's
+    per-epoch recording (xz slices of T, Q, phase and plume at mid-y: run_highres_knowledge_suite.py:280-306)."""
+    import numpy as np
+    import torch
+    from bug_defense_b200 import workloads
+    from bug_defense_b200.phase import compute_phase_map
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    eng = make_engine(geo, dev, seed_offset=101)
+    h2d = sum(np.asarray(v).nbytes for v in (geo["optical"]["mu_a"], geo["optical"]["mu_s"], geo["optical"]["g"],
+                                               geo["optical"]["n"], geo["k_grid"], geo["rho_cp_grid"],
+                                               geo["h_lat_grid"], geo["dry_mask"], geo["ablated_mask"]))
+    h2d += sum(np.asarray(geo["dry_state"][k]).nbytes for k in ("mu_a", "mu_s", "g", "n", "k", "rho_cp"))
+    my = eng.Ny // 2
+    n_on = max(1, int(round(LASER_DUTY * K)))
+    pinned = {k: torch.empty((eng.Nx, eng.Nz), dtype=dt, pin_memory=True)
+              for k, dt in (("T", torch.float32), ("Q", torch.float32), ("phase", torch.uint8), ("plume", torch.float32))}
+    d2h = 0
+    scale = POWER_W / (eng.n_photons * eng.voxel_vol)
+    for s in range(K):
+        eng.power = POWER_W if s < n_on else 0.0
+        diag = eng.step_epoch()
+        flags = eng._flags[:, my, :]
+        ph = compute_phase_map(eng._T[:, my, :], eng._chi[:, my, :], (flags & 2) != 0, (flags & 1) != 0,
+                               eng._H[:, my, :])
+        pinned["T"].copy_(eng._T[:, my, :], non_blocking=True)
+        pinned["Q"].copy_(eng._A[:, my, :] * (scale if eng.power > 0 else 0.0), non_blocking=True)
+        pinned["phase"].copy_(ph, non_blocking=True)
+        pinned["plume"].copy_(eng.plume.raw[:, my, :], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        d2h = ctypes.sizeof(__import__("bug_defense_b200")._lib.EpochDiag) + sum(
+            t.numel() * t.element_size() for t in pinned.values())
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"value": K / (ms / 1e3), "unit": "epochs/s", "h2d_bytes_per_step": int(h2d / K),
+            "d2h_bytes_per_step": int(d2h), "note": "engine construction from host arrays + per-epoch diagnostics "
+                                                     "and xz recording slices, amortised over the timed epochs"}
+
+
+def ours_main(args):
+    import torch
+    import torch.distributed as dist
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    r = run_ours(args, rank, world, local)
+    eng, geo = r["eng"], r["geo"]
+    K, ms = r["K"], r["ms"]
+    value = K * world / (ms / 1e3)
+    hbm, peak_kind, peaks = measured_peaks()
+    ab = algorithmic_bytes(geo, eng)
+    from bug_defense_b200.ablation import plume_steps_per_substep
+    n_plume_sub, _ = plume_steps_per_substep(eng._desc.plume)
+    stage = r["stage_ms"]
+    stage_names = ["mc", "substeps", "plume", "epoch_end"]
+    # dominant HBM-bound stage among the stencils
+    launches_sub = eng.n_substeps * K
+    launches_plume = eng.n_substeps * n_plume_sub * K
+    per_launch = {"substeps": stage[1] / max(launches_sub, 1), "plume": stage[2] / max(launches_plume, 1)}
+    dom = "substeps" if stage[1] >= stage[2] else "plume"
+    bytes_per_launch = ab["substep"] if dom == "substeps" else ab["plume_step"]
+    achieved = bytes_per_launch / (per_launch[dom] * 1e-3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        tj = json.loads(tf.read_text())
+        key = {"substeps": "k_substep", "plume": "k_plume_step"}[dom]
+        if key in tj:
+            traffic = tj[key]["bytes_per_voxel"] * eng.Nx * eng.Ny * eng.Nz
+    roof = {"bound": "hbm", "kernel": {"substeps": "k_substep<fused ablation>", "plume": "k_plume_step"}[dom],
+            "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+            "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+            else "fallback 6650 GB/s", "algorithmic_bytes_per_launch": bytes_per_launch,
+            "avg_launch_ms": round(per_launch[dom], 5)}
+    led = r["last_diag"]["ledger"]
+    mc_ms = stage[0]
+    photons = r["n_on"] * eng.n_photons
+    mc = {"photons_per_s": photons / (mc_ms * 1e-3) if mc_ms > 0 else None,
+          "mc_ms_per_laser_epoch": mc_ms / max(r["n_on"], 1)}
+    gpu_launches = K * (1 + 3 + eng.n_substeps + eng.n_substeps * n_plume_sub) + r["n_on"] * 2
+    out = {"metric": METRIC, "value": round(value, 3), "unit": "epochs/s", "n_gpus": world, "steps": K,
+           "warmup": args.warmup, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32 (FP64 ledgers)", "data": "synthetic (seeded, reference config shapes)",
+           "config": {"workload": "full-resolution coupled run: 200x200x128 stack + 64 plume air slices "
+                                  "(200x200x192 @ 15 um), 150k photons/laser epoch, 20 x 50 us substeps, "
+                                  f"laser on for the first {int(LASER_DUTY * 100)} % of timed epochs",
+                      "voxels": eng.Nx * eng.Ny * eng.Nz, "photons_per_laser_epoch": eng.n_photons,
+                      "plume_D_mm2_s": round(geo["plume_D"], 3), "plume_steps_per_substep": n_plume_sub,
+                      "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (>= 30 MB per field)",
+                      "seed": args.seed},
+           "stage_ms_per_epoch": {n: round(v / K, 4) for n, v in zip(stage_names, stage)},
+           "mc": mc, "roofline": roof, "clocks": r["clocks"], "gpu_launches": gpu_launches, "impl": "ours"}
+    if rank == 0 and world == 1 and not args.no_e2e:
+        import torch
+        out["e2e"] = e2e_run(args, geo, torch.device("cuda", local), K)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from bug_defense_b200.workloads import engine_kwargs
+        out["cpu_baseline"] = cpu_port_baseline(geo, engine_kwargs(geo))
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def reference_main(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from bug_defense_b200 import workloads
+    geo = workloads.full_coupled_run(seed=args.seed)
+    from bug_defense_b200.workloads import engine_kwargs
+    cb = cpu_port_baseline(geo, engine_kwargs(geo), on_epochs=1, off_epochs=1)
+    value = cb["value"]
+    out = {"metric": METRIC, "value": round(value, 5), "unit": "epochs/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": round(1e3 / value, 2), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, reference config shapes)",
+           "config": {"workload": "full-resolution coupled run: 200x200x128 stack + 64 plume air slices "
+                                  "(200x200x192 @ 15 um), 150k photons/laser epoch, 20 x 50 us substeps, "
+                                  f"laser duty {int(LASER_DUTY * 100)} %", "seed": args.seed},
+           "impl": "reference", "cpu_baseline": cb,
+           "e2e": {"value": round(value, 5), "unit": "epochs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        reference_main(a)
+    else:
+        ours_main(a)

@@ -1,0 +1,308 @@
+// Device-resident coupled epoch (CoupledAblationEngine.step_epoch,
+// simulation/coupled_ablation.py:440-617) with no host round trip inside an epoch:
+//   epoch begin  -> zero per-epoch counters, t += dt_epoch, photon-stream offset
+//   MC           -> bd_mc_trace on the packed properties of the previous epoch end
+//   substeps     -> n fused bioheat/plateau/Arrhenius/char substeps, source = A * P/(N V)
+//                   with zero source in ablated voxels (coupled_ablation.py:474-478)
+//   plume        -> transport in the void domain (dt policy: as given / Metal clamp / subcycle)
+//   epoch end    -> phase update, removal, breach, plume inject + saturation, MC properties
+// All state lives in device buffers owned by the caller; the engine owns only scratch.
+#include "engine.cuh"
+
+#include <algorithm>
+#include <vector>
+
+struct BdEngine {
+    BdEngineDesc d;
+    bd::PhaseArgs pa;
+    bd::EngineDyn* dyn = nullptr;      // device
+    bd::EngineDyn* dyn_host = nullptr; // pinned
+    unsigned long long* queue = nullptr;
+    double* partials = nullptr;
+    int partial_blocks = 0;
+    int sm_count = 148;
+    long long epochs_enqueued = 0;  // host mirror of the epoch count (photon-stream offsets)
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool timed = false;
+    // stage-timing ring: 5 events per timed epoch
+    bool ring_on = false;
+    std::vector<cudaEvent_t> ring;
+    size_t ring_used = 0;
+    int ring_error = 0;
+};
+
+static cudaEvent_t ring_event(BdEngine* e) {
+    if (e->ring_used == e->ring.size()) {
+        cudaEvent_t ev = nullptr;
+        if (cudaEventCreate(&ev) != cudaSuccess) {
+            e->ring_error = 1;
+            return nullptr;
+        }
+        e->ring.push_back(ev);
+    }
+    return e->ring[e->ring_used++];
+}
+
+static void mark(BdEngine* e, cudaStream_t st, int slot) {
+    if (e->timed && slot >= 0 && slot < 4 && slot != 3) cudaEventRecord(e->ev[slot], st);
+    if (e->ring_on && e->timed) {
+        cudaEvent_t ev = ring_event(e);
+        if (ev) cudaEventRecord(ev, st);
+    }
+}
+
+namespace bd {
+
+__global__ void k_epoch_begin(EngineDyn* dyn, double dt_epoch) {
+    if (threadIdx.x < BD_LEDGER_LEN) dyn->ledger[threadIdx.x] = 0.0;
+    if (threadIdx.x == 0) {
+        dyn->n_new = 0ull;
+        dyn->gap_open = 0u;
+        dyn->plume_peak_bits = 0u;
+        dyn->plume_tau_sum = 0.0;
+        dyn->plume_abl_sum = 0.0;
+        dyn->n_ablated = 0.0;
+        dyn->epoch += 1;
+        dyn->t += dt_epoch;
+        dyn->t_now = (float)dyn->t;
+        dyn->mc_offset = dyn->epoch << 32;
+    }
+}
+
+__global__ void k_epoch_end_only(EngineDyn* dyn) {
+    if (threadIdx.x == 0) {
+        dyn->n_new = 0ull;
+        dyn->gap_open = 0u;
+        dyn->plume_peak_bits = 0u;
+        dyn->plume_tau_sum = 0.0;
+        dyn->plume_abl_sum = 0.0;
+        dyn->n_ablated = 0.0;
+        dyn->t_now = (float)dyn->t;
+    }
+}
+
+__global__ void k_set_time(EngineDyn* dyn, double t, long long epoch) {
+    dyn->t = t;
+    dyn->epoch = epoch;
+    dyn->t_now = (float)t;
+}
+
+static GridRef gref(const BdGridRef& r) { return GridRef{r.ptr, r.value}; }
+
+static PhaseArgs phase_args(const BdPhaseDesc& p, EngineDyn* dyn) {
+    PhaseArgs a;
+    a.nx = p.nx; a.ny = p.ny; a.nz = p.nz;
+    a.single_stage = p.single_stage; a.apply_removal = p.apply_removal;
+    a.has_cs = p.has_char_state; a.has_cs_mu_a = p.has_cs_mu_a; a.has_cs_mu_s = p.has_cs_mu_s;
+    a.has_cs_k = p.has_cs_k; a.has_cs_rho = p.has_cs_rho_cp;
+    a.gap_k0 = p.gap_k0; a.gap_k1 = p.gap_k1; a.has_plume = p.has_plume;
+    a.t_abl = p.t_abl; a.alpha_max = p.alpha_max_stable; a.cs_chi_rem = p.cs_chi_remove;
+    a.k_void = p.k_void; a.rho_void = p.rho_cp_void; a.t_void = p.t_void;
+    a.delta_mu = p.plume_delta_mu; a.mu_max = p.plume_mu_max; a.ratio_a = p.plume_ratio_a;
+    a.ratio_s = p.plume_ratio_s; a.g_plume = p.plume_g;
+    a.T = p.T; a.H = p.H_acc; a.chi = p.chi; a.mu_a = p.mu_a; a.mu_s = p.mu_s; a.g = p.g; a.n = p.n;
+    a.k = p.k; a.rho = p.rho_cp; a.T_peak = p.T_peak; a.ablation_time = p.ablation_time;
+    a.h_lat = p.h_lat; a.wet_mu_a = p.wet_mu_a; a.wet_k = p.wet_k; a.wet_rho = p.wet_rho_cp;
+    a.ds_mu_a = gref(p.ds_mu_a); a.ds_mu_s = gref(p.ds_mu_s); a.ds_g = gref(p.ds_g); a.ds_n = gref(p.ds_n);
+    a.ds_k = gref(p.ds_k); a.ds_rho = gref(p.ds_rho_cp); a.ds_t_rem = gref(p.ds_t_remove);
+    a.cs_mu_a = gref(p.cs_mu_a); a.cs_mu_s = gref(p.cs_mu_s); a.cs_k = gref(p.cs_k); a.cs_rho = gref(p.cs_rho_cp);
+    a.cs_t_rem = gref(p.cs_t_remove);
+    a.flags = p.flags; a.to_remove = p.to_remove; a.plume = p.plume; a.mu_ext = p.mu_ext; a.props = p.props;
+    a.dyn = dyn;
+    return a;
+}
+
+static int validate(const BdEngineDesc* d) {
+    const BdPhaseDesc& p = d->phase;
+    BD_REQUIRE(p.nx > 0 && p.ny > 0 && p.nz > 0, "bd_engine_create: grid dims must be positive");
+    BD_REQUIRE(p.T && p.H_acc && p.mu_a && p.mu_s && p.g && p.n && p.k && p.rho_cp && p.flags && p.h_lat,
+               "bd_engine_create: missing state field");
+    BD_REQUIRE(p.single_stage || (p.wet_mu_a && p.wet_k && p.wet_rho_cp),
+               "bd_engine_create: dry_state needs the wet property copies");
+    BD_REQUIRE(!p.has_plume || (p.plume && p.mu_ext), "bd_engine_create: plume needs raw and extinction fields");
+    BD_REQUIRE(p.gap_k0 <= 0 || (p.gap_k0 < p.gap_k1 && p.gap_k1 <= p.nz), "bd_engine_create: bad air_gap_range");
+    BD_REQUIRE(d->n_substeps >= 0, "bd_engine_create: n_substeps must be >= 0");
+    BD_REQUIRE(d->T_alt != nullptr, "bd_engine_create: T_alt is required");
+    BD_REQUIRE(!d->has_plume_transport || (d->plume_alt && p.plume), "bd_engine_create: plume transport fields");
+    BD_REQUIRE(!d->substep.has_arrhenius || d->omega, "bd_engine_create: Arrhenius needs omega");
+    BD_REQUIRE(!d->substep.has_char || p.chi, "bd_engine_create: char kinetics need chi");
+    BD_REQUIRE(d->A != nullptr, "bd_engine_create: absorbed map A is required");
+    BD_REQUIRE(d->voxel_volume > 0.0, "bd_engine_create: voxel_volume must be > 0");
+    return BD_OK;
+}
+
+}  // namespace bd
+
+using namespace bd;
+
+extern "C" int bd_engine_create(const BdEngineDesc* desc, BdEngine** out) {
+    BD_REQUIRE(desc && out, "bd_engine_create: NULL argument");
+    int rc = validate(desc);
+    if (rc) return rc;
+    BdEngine* e = new BdEngine();
+    e->d = *desc;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&e->sm_count, cudaDevAttrMultiProcessorCount, dev);
+    e->partial_blocks = e->sm_count * 16;
+    cudaError_t err = cudaMalloc(&e->dyn, sizeof(EngineDyn));
+    if (err == cudaSuccess) err = cudaMallocHost(&e->dyn_host, sizeof(EngineDyn));
+    if (err == cudaSuccess) err = cudaMalloc(&e->queue, sizeof(unsigned long long));
+    if (err == cudaSuccess) err = cudaMalloc(&e->partials, sizeof(double) * BD_LEDGER_LEN * e->partial_blocks);
+    if (err == cudaSuccess) err = cudaMemset(e->dyn, 0, sizeof(EngineDyn));
+    for (int q = 0; q < 4 && err == cudaSuccess; ++q) err = cudaEventCreate(&e->ev[q]);
+    if (err != cudaSuccess) {
+        bd_engine_destroy(e);
+        return cuda_status(err, "bd_engine_create");
+    }
+    e->pa = phase_args(desc->phase, e->dyn);
+    *out = e;
+    return BD_OK;
+}
+
+extern "C" int bd_engine_destroy(BdEngine* e) {
+    if (!e) return BD_OK;
+    cudaFree(e->dyn);
+    cudaFreeHost(e->dyn_host);
+    cudaFree(e->queue);
+    cudaFree(e->partials);
+    for (int q = 0; q < 4; ++q)
+        if (e->ev[q]) cudaEventDestroy(e->ev[q]);
+    for (cudaEvent_t ev : e->ring) cudaEventDestroy(ev);
+    delete e;
+    return BD_OK;
+}
+
+extern "C" int bd_engine_set_time(BdEngine* e, double t, int64_t epoch, void* stream) {
+    BD_REQUIRE(e != nullptr, "bd_engine_set_time: NULL engine");
+    k_set_time<<<1, 1, 0, as_stream(stream)>>>(e->dyn, t, (long long)epoch);
+    e->epochs_enqueued = (long long)epoch;
+    BD_CHECK_LAUNCH("k_set_time");
+    return BD_OK;
+}
+
+extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void* stream) {
+    BD_REQUIRE(e != nullptr, "bd_engine_step_epoch: NULL engine");
+    BD_REQUIRE(power >= 0.0f, "bd_engine_step_epoch: power must be >= 0");
+    cudaStream_t st = as_stream(stream);
+    const BdEngineDesc& d = e->d;
+    const long long nv = (long long)d.phase.nx * d.phase.ny * d.phase.nz;
+    k_epoch_begin<<<1, 32, 0, st>>>(e->dyn, d.dt_epoch);
+    BD_CHECK_LAUNCH("k_epoch_begin");
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cap);
+    e->timed = (cap == cudaStreamCaptureStatusNone);
+    mark(e, st, 0);
+
+    const bool laser = power > 0.0f;
+    if (laser && !(options & BD_EPOCH_SKIP_MC)) {
+        BD_REQUIRE(d.phase.props != nullptr, "bd_engine_step_epoch: MC needs the packed property buffer");
+        BD_CUDA(cudaMemsetAsync(d.A, 0, sizeof(float) * nv, st));
+        if (d.L && (d.mc.options & BD_MC_TALLY_FLUENCE)) BD_CUDA(cudaMemsetAsync(d.L, 0, sizeof(float) * nv, st));
+        BdMcParams mp = d.mc;
+        // one 2^32 photon-index window per epoch keeps every epoch's Philox streams distinct
+        mp.photon_offset = (int64_t)(++e->epochs_enqueued) << 32;
+        int rc = mc_launch(&mp, d.phase.props, d.phase.flags, d.A, d.L, d.lat_depth, e->dyn->ledger, e->queue,
+                           e->partials, e->partial_blocks, e->sm_count, st);
+        if (rc) return rc;
+    } else {
+        ++e->epochs_enqueued;
+    }
+
+    mark(e, st, 1);
+    if (d.n_substeps > 0) {
+        BdAblationParams ap = d.substep;
+        ap.is_active = laser ? 1 : 0;
+        ap.q_scale = (d.mc.n_photons > 0) ? (float)((double)power / ((double)d.mc.n_photons * d.voxel_volume)) : 0.0f;
+        ap.zero_src_in_ablated = 1;
+        int rc = ablation_launch(&ap, d.phase.T, d.T_alt, d.n_substeps, d.phase.H_acc, d.omega, d.phase.chi,
+                                 d.phase.flags, d.A, d.phase.k, d.phase.rho_cp, st);
+        if (rc) return rc;
+        if (d.n_substeps & 1) BD_CUDA(cudaMemcpyAsync(d.phase.T, d.T_alt, sizeof(float) * nv, cudaMemcpyDeviceToDevice, st));
+    }
+    mark(e, st, -1);
+    if (d.n_substeps > 0) {
+        if (d.has_plume_transport) {
+            int in_b = 0;
+            int rc = plume_launch(&d.plume, d.phase.plume, d.plume_alt, d.n_substeps, d.phase.flags, &in_b, st);
+            if (rc) return rc;
+            if (in_b)
+                BD_CUDA(cudaMemcpyAsync(d.phase.plume, d.plume_alt, sizeof(float) * nv, cudaMemcpyDeviceToDevice, st));
+        }
+    }
+    mark(e, st, 2);
+    int rc = phase_launch(e->pa, 1, st);
+    if (e->timed) cudaEventRecord(e->ev[3], st);
+    if (e->ring_on && e->timed) {
+        cudaEvent_t ev = ring_event(e);
+        if (ev) cudaEventRecord(ev, st);
+    }
+    return rc;
+}
+
+extern "C" int bd_engine_set_mc(BdEngine* e, const BdMcParams* mc) {
+    BD_REQUIRE(e && mc, "bd_engine_set_mc: NULL argument");
+    BD_REQUIRE(mc->nx == e->d.phase.nx && mc->ny == e->d.phase.ny && mc->nz == e->d.phase.nz,
+               "bd_engine_set_mc: grid differs from the engine's");
+    e->d.mc = *mc;
+    return BD_OK;
+}
+
+extern "C" int bd_engine_timing(BdEngine* e, int enable) {
+    BD_REQUIRE(e != nullptr, "bd_engine_timing: NULL engine");
+    e->ring_on = enable != 0;
+    e->ring_used = 0;
+    e->ring_error = 0;
+    return BD_OK;
+}
+
+extern "C" int bd_engine_timing_read(BdEngine* e, double* stage_ms, int64_t* epochs) {
+    BD_REQUIRE(e && stage_ms && epochs, "bd_engine_timing_read: NULL argument");
+    if (e->ring_error) return fail(BD_ERR_OUT_OF_MEMORY, "bd_engine_timing_read: event creation failed");
+    for (int q = 0; q < 4; ++q) stage_ms[q] = 0.0;
+    const size_t n = e->ring_used / 5;
+    *epochs = (int64_t)n;
+    if (n == 0) return BD_OK;
+    BD_CUDA(cudaEventSynchronize(e->ring[e->ring_used - 1]));
+    for (size_t ep = 0; ep < n; ++ep)
+        for (int q = 0; q < 4; ++q) {
+            float ms = 0.0f;
+            BD_CUDA(cudaEventElapsedTime(&ms, e->ring[ep * 5 + q], e->ring[ep * 5 + q + 1]));
+            stage_ms[q] += ms;
+        }
+    return BD_OK;
+}
+
+extern "C" int bd_engine_epoch_end(BdEngine* e, void* stream) {
+    BD_REQUIRE(e != nullptr, "bd_engine_epoch_end: NULL engine");
+    cudaStream_t st = as_stream(stream);
+    k_epoch_end_only<<<1, 32, 0, st>>>(e->dyn);
+    BD_CHECK_LAUNCH("k_epoch_end_only");
+    return phase_launch(e->pa, 1, st);
+}
+
+extern "C" int bd_engine_read_diag(BdEngine* e, BdEpochDiag* out, void* stream) {
+    BD_REQUIRE(e && out, "bd_engine_read_diag: NULL argument");
+    cudaStream_t st = as_stream(stream);
+    BD_CUDA(cudaMemcpyAsync(e->dyn_host, e->dyn, sizeof(EngineDyn), cudaMemcpyDeviceToHost, st));
+    BD_CUDA(cudaStreamSynchronize(st));
+    const EngineDyn& h = *e->dyn_host;
+    for (int q = 0; q < BD_LEDGER_LEN; ++q) out->ledger[q] = h.ledger[q];
+    out->epoch = (double)h.epoch;
+    out->time_s = h.t;
+    out->n_new = (double)h.n_new;
+    out->n_ablated = h.n_ablated;
+    out->gap_open = (double)h.gap_open;
+    out->plume_tau = h.plume_tau_sum * (double)e->d.plume.dz;
+    out->plume_peak_mu_a = (double)__builtin_bit_cast(float, h.plume_peak_bits);
+    out->plume_ablated_sum = h.plume_abl_sum;
+    out->t_optical_ms = out->t_thermal_ms = out->t_epoch_end_ms = 0.0;
+    if (e->timed) {
+        float a = 0, b = 0, c = 0;
+        if (cudaEventElapsedTime(&a, e->ev[0], e->ev[1]) == cudaSuccess) out->t_optical_ms = a;
+        if (cudaEventElapsedTime(&b, e->ev[1], e->ev[2]) == cudaSuccess) out->t_thermal_ms = b;
+        if (cudaEventElapsedTime(&c, e->ev[2], e->ev[3]) == cudaSuccess) out->t_epoch_end_ms = c;
+        cudaGetLastError();
+    }
+    return BD_OK;
+}

@@ -1,0 +1,58 @@
+// Internal structures shared by the epoch-end kernels and the engine orchestration.
+#pragma once
+
+#include "common.cuh"
+
+namespace bd {
+
+struct GridRef {
+    const float* ptr;  // per-voxel values, or nullptr to use `value`
+    float value;
+};
+
+// Device-resident per-epoch scalars (zeroed at the start of every epoch except t/epoch).
+struct EngineDyn {
+    double ledger[BD_LEDGER_LEN];
+    unsigned long long n_new;
+    unsigned int gap_open;
+    unsigned int plume_peak_bits;
+    double plume_tau_sum;
+    double plume_abl_sum;
+    double n_ablated;
+    double t;             // simulated time after this epoch
+    long long epoch;      // epochs completed
+    float t_now;          // t as float for the kernels
+    float _pad;
+    long long mc_offset;  // photon-stream offset of this epoch's MC
+};
+
+struct PhaseArgs {
+    int nx, ny, nz;
+    int single_stage, apply_removal;
+    int has_cs, has_cs_mu_a, has_cs_mu_s, has_cs_k, has_cs_rho;
+    int gap_k0, gap_k1;
+    int has_plume;
+    float t_abl, alpha_max, cs_chi_rem, k_void, rho_void, t_void;
+    float delta_mu, mu_max, ratio_a, ratio_s, g_plume;
+    float *T, *H, *chi, *mu_a, *mu_s, *g, *n, *k, *rho, *T_peak, *ablation_time;
+    const float *h_lat, *wet_mu_a, *wet_k, *wet_rho;
+    GridRef ds_mu_a, ds_mu_s, ds_g, ds_n, ds_k, ds_rho, ds_t_rem;
+    GridRef cs_mu_a, cs_mu_s, cs_k, cs_rho, cs_t_rem;
+    uint8_t* flags;
+    uint8_t* to_remove;   // optional per-voxel output
+    float *plume, *mu_ext;
+    float* props;         // float4 per voxel, optional
+    EngineDyn* dyn;
+};
+
+int phase_launch(const PhaseArgs& a, int with_plume_pass, cudaStream_t st);
+int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, float* H, float* Om, float* Chi,
+                    const uint8_t* F, const float* src, const float* K, const float* R, cudaStream_t st);
+int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
+                 cudaStream_t st);
+int plume_policy_steps(const BdPlumeParams* p, int* n_steps, float* dt_step, float* decay_step);
+int mc_launch(const BdMcParams* p, const float* props, const uint8_t* flags, float* A, float* L, double* latz,
+              double* ledger, unsigned long long* queue, double* partials, int max_blocks, int sm_count,
+              cudaStream_t st);
+
+}  // namespace bd

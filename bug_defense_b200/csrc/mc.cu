@@ -1,0 +1,553 @@
+// Voxel Monte Carlo photon transport (hop-drop-spin with optical-depth voxel marching).
+//
+// Algorithm follows the reference CPU tracer simulation/voxel_mc_3d.py:123-337
+// (_trace_one_photon) and its Metal twin simulation/voxel_mc_metal.py:173-332:
+//   launch (Gaussian / top-hat / Kim disks, oblique footprint stretch u1/cos(theta))
+//   -> deterministic entrance Fresnel split + Snell refraction
+//   -> loop: tau = -ln(xi) consumed voxel by voxel; collision absorbs w*mu_a/mu_t,
+//      Russian roulette at w < 1e-4 (survive 1/10 with w*10), Henyey-Greenstein scatter;
+//      face crossings do Fresnel/TIR or Snell at index steps, exits tally R_diff / T / lateral.
+//
+// B200 design:
+//   * one persistent grid, photons handed out by a global atomic queue so warps stay full
+//     while the per-photon step counts differ by orders of magnitude;
+//   * Philox-4x32-10 counter-based RNG keyed on (seed, photon index): no RNG state in memory
+//     and a photon's path does not depend on which thread traced it;
+//   * optical properties packed as one float4 {mu_t, mu_a/mu_t, g, n} per voxel read through
+//     the read-only (L1/texture) path: one 16-byte load per event;
+//   * absorbed weight and track length tallied with fire-and-forget FP32 reductions;
+//   * FP64 ledger: per-thread FP64 registers for the per-event channels, per-block shared
+//     accumulators for per-photon channels, one partial per block reduced in a fixed order.
+#include "common.cuh"
+
+#include <stdlib.h>
+
+namespace bd {
+
+struct McDev {
+    int nx, ny, nz, launch_axis;
+    float dx, dy, dz, lx, ly, lz;
+    float ux0, uy0, uz0, cos_ph, sin_ph, cos_th_safe;
+    float xc, yc, zc, sigma, radius;
+    int profile;
+    float n_amb, rmax2;
+    int options;
+    long long n_photons, offset, max_events;
+    unsigned long long seed;
+    float eq_eps;     // Fresnel index-equality guard
+    float step_eps;   // internal index-step threshold
+    float entry_eps;  // entrance refraction threshold
+};
+
+__device__ __forceinline__ float fresnel_unpol(float n1, float n2, float cos_i, float eq_eps) {
+    // voxel_mc_3d.py:33-48 / voxel_mc_metal.py:70-83
+    if (fabsf(n1 - n2) < eq_eps) return 0.0f;
+    cos_i = fminf(1.0f, fabsf(cos_i));
+    if (cos_i > 0.999999f) {
+        float r = (n1 - n2) / (n1 + n2);
+        return r * r;
+    }
+    float q = n1 / n2;
+    float sin_t2 = q * q * (1.0f - cos_i * cos_i);
+    if (sin_t2 >= 1.0f) return 1.0f;
+    float cos_t = sqrtf(1.0f - sin_t2);
+    float a = n1 * cos_i, b = n2 * cos_t, c = n1 * cos_t, d = n2 * cos_i;
+    float rs = (a - b) / (a + b);
+    float rp = (c - d) / (c + d);
+    return 0.5f * (rs * rs + rp * rp);
+}
+
+// Snell refraction across an axis-aligned face (voxel_mc_3d.py:51-69)
+__device__ __forceinline__ void refract_axis(float& ux, float& uy, float& uz, int axis, float eta) {
+    if (axis == 0) {
+        float s = ux > 0.0f ? 1.0f : -1.0f;
+        uy *= eta; uz *= eta;
+        ux = s * sqrtf(fmaxf(0.0f, 1.0f - uy * uy - uz * uz));
+    } else if (axis == 1) {
+        float s = uy > 0.0f ? 1.0f : -1.0f;
+        ux *= eta; uz *= eta;
+        uy = s * sqrtf(fmaxf(0.0f, 1.0f - ux * ux - uz * uz));
+    } else {
+        float s = uz > 0.0f ? 1.0f : -1.0f;
+        ux *= eta; uy *= eta;
+        uz = s * sqrtf(fmaxf(0.0f, 1.0f - ux * ux - uy * uy));
+    }
+}
+
+// Henyey-Greenstein deflection + uniform azimuth (voxel_mc_3d.py:229-262)
+__device__ __forceinline__ void scatter_hg(float& ux, float& uy, float& uz, float g, PhotonRng& rng) {
+    float xi = rng.uniform();
+    float cost;
+    if (fabsf(g) < 1e-4f) {
+        cost = 2.0f * xi - 1.0f;
+    } else {
+        float t = (1.0f - g * g) / (1.0f - g + 2.0f * g * xi);
+        cost = (1.0f + g * g - t * t) / (2.0f * g);
+        cost = fminf(1.0f, fmaxf(-1.0f, cost));
+    }
+    float sint = sqrtf(fmaxf(0.0f, 1.0f - cost * cost));
+    float sinp, cosp;
+    sincospif(2.0f * rng.uniform(), &sinp, &cosp);
+    float nx, ny, nz;
+    if (fabsf(uz) > 0.99999f) {
+        float sz = uz > 0.0f ? 1.0f : -1.0f;
+        nx = sint * cosp;
+        ny = sint * sinp;
+        nz = cost * sz;
+    } else {
+        float den = sqrtf(fmaxf(1.0f - uz * uz, 1e-12f));
+        float f = sint / den;
+        nx = f * (ux * uz * cosp - uy * sinp) + ux * cost;
+        ny = f * (uy * uz * cosp + ux * sinp) + uy * cost;
+        nz = -sint * cosp * den + uz * cost;
+    }
+    float nn = nx * nx + ny * ny + nz * nz;
+    if (nn > 1e-24f) {
+        float r = rsqrtf(nn);
+        nx *= r; ny *= r; nz *= r;
+    }
+    ux = nx; uy = ny; uz = nz;
+}
+
+// Transverse launch offsets (voxel_mc_3d.py:101-120)
+__device__ __forceinline__ void beam_offsets(const McDev& P, PhotonRng& rng, float& u1, float& u2) {
+    if (P.profile == BD_BEAM_TOPHAT) {
+        float r = P.radius * sqrtf(rng.uniform());
+        float s, c;
+        sincospif(2.0f * rng.uniform(), &s, &c);
+        u1 = r * c; u2 = r * s;
+        return;
+    }
+    if (P.profile == BD_BEAM_KIM_EXP_DISK || P.profile == BD_BEAM_KIM_GAUSS_DISK) {
+        float rn = 0.0f;
+        // rejection sampling; acceptance >= e^-2, so 256 tries all fail with p < 1e-16
+        for (int t = 0; t < 256; ++t) {
+            rn = sqrtf(rng.uniform());
+            float acc = (P.profile == BD_BEAM_KIM_EXP_DISK) ? expf(-2.0f * rn) : expf(-2.0f * rn * rn);
+            if (rng.uniform() < acc) break;
+        }
+        float s, c;
+        sincospif(2.0f * rng.uniform(), &s, &c);
+        u1 = P.radius * rn * c; u2 = P.radius * rn * s;
+        return;
+    }
+    // Gaussian: Box-Muller pair with per-axis sigma
+    float a = rng.uniform_pos();
+    float b = rng.uniform();
+    float r = sqrtf(-2.0f * logf(a)) * P.sigma;
+    float s, c;
+    sincospif(2.0f * b, &s, &c);
+    u1 = r * c; u2 = r * s;
+}
+
+struct ThreadLedger {
+    double absorbed, absorbed_void, gain;
+    unsigned long long collisions, crossings, reflections;
+};
+
+template <int DEPTH>  // 2: launch along +z at z=0 ; 0: launch along +x at x=0
+__device__ __forceinline__ void trace_photon(const McDev& P, long long pid, const float4* __restrict__ props,
+                                             const uint8_t* __restrict__ flags, float* __restrict__ A,
+                                             float* __restrict__ L, double* __restrict__ latz,
+                                             double* sl, ThreadLedger& tl) {
+    PhotonRng rng;
+    rng.init(P.seed, (unsigned long long)(P.offset + pid));
+    const bool metal = (P.options & BD_MC_METAL_SEMANTICS) != 0;
+    const bool tally_l = (P.options & BD_MC_TALLY_FLUENCE) != 0 && L != nullptr;
+
+    float u1, u2;
+    beam_offsets(P, rng, u1, u2);
+    float x, y, z;
+    int ix, iy, iz;
+    const float stretch = u1 / P.cos_th_safe;
+    if (DEPTH == 2) {
+        x = P.xc + stretch * P.cos_ph - u2 * P.sin_ph;
+        y = P.yc + stretch * P.sin_ph + u2 * P.cos_ph;
+        z = 0.0f;
+        bool out = x < 0.0f || x >= P.lx || y < 0.0f || y >= P.ly;
+        if (!out && P.rmax2 > 0.0f) {
+            float a = x - P.xc, b = y - P.yc;
+            out = a * a + b * b >= P.rmax2;
+        }
+        if (out) {
+            atomicAdd(&sl[BD_LEDGER_LATERAL], 1.0);
+            if (latz) atomicAdd(&latz[0], 1.0);
+            return;
+        }
+        ix = min((int)(x / P.dx), P.nx - 1);
+        iy = min((int)(y / P.dy), P.ny - 1);
+        iz = 0;
+    } else {
+        x = 0.0f;
+        y = P.yc + stretch * P.cos_ph - u2 * P.sin_ph;
+        z = P.zc + stretch * P.sin_ph + u2 * P.cos_ph;
+        bool out = y < 0.0f || y >= P.ly || z < 0.0f || z >= P.lz;
+        if (!out && P.rmax2 > 0.0f) {
+            float a = y - P.yc, b = z - P.zc;
+            out = a * a + b * b >= P.rmax2;
+        }
+        if (out) {
+            atomicAdd(&sl[BD_LEDGER_LATERAL], 1.0);
+            if (latz) atomicAdd(&latz[0], 1.0);
+            return;
+        }
+        ix = 0;
+        iy = min((int)(y / P.dy), P.ny - 1);
+        iz = min((int)(z / P.dz), P.nz - 1);
+    }
+    float ux = P.ux0, uy = P.uy0, uz = P.uz0;
+    const int ny = P.ny, nz = P.nz;
+    const size_t sx_stride = (size_t)ny * nz;
+    size_t idx = (size_t)ix * sx_stride + (size_t)iy * nz + iz;
+
+    // entrance face: deterministic specular split + refraction (voxel_mc_3d.py:183-192)
+    float4 pr = __ldg(&props[idx]);
+    float w;
+    {
+        float n_in = pr.w;
+        float cos_in = (DEPTH == 2) ? uz : ux;
+        float r = fresnel_unpol(P.n_amb, n_in, cos_in, P.eq_eps);
+        atomicAdd(&sl[BD_LEDGER_SPECULAR], (double)r);
+        w = 1.0f - r;
+        if (w <= 0.0f) return;
+        if (fabsf(n_in - P.n_amb) > P.entry_eps) refract_axis(ux, uy, uz, DEPTH, P.n_amb / n_in);
+    }
+    float iux = fabsf(ux) > 1e-15f ? 1.0f / ux : 0.0f;
+    float iuy = fabsf(uy) > 1e-15f ? 1.0f / uy : 0.0f;
+    float iuz = fabsf(uz) > 1e-15f ? 1.0f / uz : 0.0f;
+    float tau = -__logf(fmaxf(rng.uniform(), 1e-12f));
+
+    const float dx = P.dx, dy = P.dy, dz = P.dz;
+    unsigned long long ncol = 0, ncross = 0, nrefl = 0;
+    long long ev = 0;
+    for (; ev < P.max_events; ++ev) {
+        // exact ray/box distance to the exit face (voxel_mc_3d.py:72-98)
+        float sx = ux > 1e-15f ? ((float)(ix + 1) * dx - x) * iux : (ux < -1e-15f ? ((float)ix * dx - x) * iux : 1e30f);
+        float sy = uy > 1e-15f ? ((float)(iy + 1) * dy - y) * iuy : (uy < -1e-15f ? ((float)iy * dy - y) * iuy : 1e30f);
+        float sz = uz > 1e-15f ? ((float)(iz + 1) * dz - z) * iuz : (uz < -1e-15f ? ((float)iz * dz - z) * iuz : 1e30f);
+        int axis;
+        float s_exit;
+        if (sx <= sy && sx <= sz) { axis = 0; s_exit = fmaxf(sx, 0.0f); }
+        else if (sy <= sz)        { axis = 1; s_exit = fmaxf(sy, 0.0f); }
+        else                      { axis = 2; s_exit = fmaxf(sz, 0.0f); }
+        const float mu_t = pr.x;
+
+        if (mu_t > 1e-12f && mu_t * s_exit >= tau) {
+            // ---- interaction inside the voxel ----
+            ++ncol;
+            float s = tau / mu_t;
+            if (tally_l) atomicAdd(&L[idx], w * s);
+            x += s * ux; y += s * uy; z += s * uz;
+            if (P.rmax2 > 0.0f) {
+                float a = (DEPTH == 2) ? x - P.xc : y - P.yc;
+                float b = (DEPTH == 2) ? y - P.yc : z - P.zc;
+                if (a * a + b * b >= P.rmax2) {
+                    atomicAdd(&sl[BD_LEDGER_LATERAL], (double)w);
+                    if (latz) atomicAdd(&latz[DEPTH == 2 ? iz : ix], (double)w);
+                    goto done;
+                }
+            }
+            {
+                float dw = w * pr.y;
+                w -= dw;
+                atomicAdd(&A[idx], dw);
+                if (flags != nullptr && (__ldg(&flags[idx]) & BD_FLAG_ABLATED)) tl.absorbed_void += (double)dw;
+                else tl.absorbed += (double)dw;
+            }
+            if (w < 1e-4f) {
+                if (rng.uniform() < 0.1f) {
+                    tl.gain += 9.0 * (double)w;
+                    w *= 10.0f;
+                } else {
+                    atomicAdd(&sl[BD_LEDGER_ROULETTE_LOSS], (double)w);
+                    goto done;
+                }
+            }
+            scatter_hg(ux, uy, uz, pr.z, rng);
+            iux = fabsf(ux) > 1e-15f ? 1.0f / ux : 0.0f;
+            iuy = fabsf(uy) > 1e-15f ? 1.0f / uy : 0.0f;
+            iuz = fabsf(uz) > 1e-15f ? 1.0f / uz : 0.0f;
+            tau = -__logf(fmaxf(rng.uniform(), 1e-12f));
+            continue;
+        }
+
+        // ---- traverse the chord and land exactly on the exit face ----
+        ++ncross;
+        tau -= mu_t * s_exit;
+        if (tally_l) atomicAdd(&L[idx], w * s_exit);
+        x += s_exit * ux; y += s_exit * uy; z += s_exit * uz;
+        int jx = ix, jy = iy, jz = iz;
+        if (axis == 0)      { int sd = ux > 0.0f ? 1 : -1; jx += sd; x = sd > 0 ? (float)(ix + 1) * dx : (float)ix * dx; }
+        else if (axis == 1) { int sd = uy > 0.0f ? 1 : -1; jy += sd; y = sd > 0 ? (float)(iy + 1) * dy : (float)iy * dy; }
+        else                { int sd = uz > 0.0f ? 1 : -1; jz += sd; z = sd > 0 ? (float)(iz + 1) * dz : (float)iz * dz; }
+
+        if (axis == DEPTH) {
+            const int jd = (DEPTH == 2) ? jz : jx;
+            const int nd = (DEPTH == 2) ? P.nz : P.nx;
+            if (jd < 0) {
+                // leaving through the entrance face: Fresnel / TIR against ambient
+                float cos_out = (DEPTH == 2) ? uz : ux;
+                float r = fresnel_unpol(pr.w, P.n_amb, cos_out, P.eq_eps);
+                if (r > 0.0f && rng.uniform() < r) {
+                    ++nrefl;
+                    if (DEPTH == 2) { uz = -uz; iuz = -iuz; } else { ux = -ux; iux = -iux; }
+                    continue;
+                }
+                atomicAdd(&sl[BD_LEDGER_DIFFUSE], (double)w);
+                goto done;
+            }
+            if (jd >= nd) {
+                atomicAdd(&sl[BD_LEDGER_TRANSMITTED], (double)w);
+                goto done;
+            }
+        } else if (jx < 0 || jx >= P.nx || jy < 0 || jy >= P.ny || jz < 0 || jz >= P.nz) {
+            atomicAdd(&sl[BD_LEDGER_LATERAL], (double)w);
+            if (latz) atomicAdd(&latz[DEPTH == 2 ? iz : ix], (double)w);
+            goto done;
+        }
+        if (!metal && P.rmax2 > 0.0f) {
+            float a = (DEPTH == 2) ? x - P.xc : y - P.yc;
+            float b = (DEPTH == 2) ? y - P.yc : z - P.zc;
+            if (a * a + b * b >= P.rmax2) {
+                atomicAdd(&sl[BD_LEDGER_LATERAL], (double)w);
+                if (latz) atomicAdd(&latz[DEPTH == 2 ? iz : ix], (double)w);
+                goto done;
+            }
+        }
+        {
+            size_t jidx = (size_t)jx * sx_stride + (size_t)jy * nz + jz;
+            float4 pn = __ldg(&props[jidx]);
+            float n1 = pr.w, n2 = pn.w;
+            if (fabsf(n1 - n2) > P.step_eps) {
+                float cos_face = axis == 0 ? ux : (axis == 1 ? uy : uz);
+                float r = fresnel_unpol(n1, n2, cos_face, P.eq_eps);
+                if ((!metal || r > 0.0f) && rng.uniform() < r) {
+                    ++nrefl;
+                    if (axis == 0) { ux = -ux; iux = -iux; }
+                    else if (axis == 1) { uy = -uy; iuy = -iuy; }
+                    else { uz = -uz; iuz = -iuz; }
+                    continue;
+                }
+                refract_axis(ux, uy, uz, axis, n1 / n2);
+                iux = fabsf(ux) > 1e-15f ? 1.0f / ux : 0.0f;
+                iuy = fabsf(uy) > 1e-15f ? 1.0f / uy : 0.0f;
+                iuz = fabsf(uz) > 1e-15f ? 1.0f / uz : 0.0f;
+            }
+            ix = jx; iy = jy; iz = jz;
+            idx = jidx;
+            pr = pn;
+        }
+    }
+    // event cap reached: the remaining weight is accounted, not lost
+    atomicAdd(&sl[BD_LEDGER_TRUNCATED], (double)w);
+done:
+    tl.collisions += ncol;
+    tl.crossings += ncross;
+    tl.reflections += nrefl;
+}
+
+template <int DEPTH>
+__global__ void __launch_bounds__(128) k_mc_trace(McDev P, const float4* __restrict__ props,
+                                                  const uint8_t* __restrict__ flags, float* __restrict__ A,
+                                                  float* __restrict__ L, double* __restrict__ latz,
+                                                  unsigned long long* __restrict__ queue,
+                                                  double* __restrict__ partials) {
+    __shared__ double sl[BD_LEDGER_LEN];
+    if (threadIdx.x < BD_LEDGER_LEN) sl[threadIdx.x] = 0.0;
+    __syncthreads();
+    ThreadLedger tl;
+    tl.absorbed = tl.absorbed_void = tl.gain = 0.0;
+    tl.collisions = tl.crossings = tl.reflections = 0ull;
+
+    const unsigned long long N = (unsigned long long)P.n_photons;
+    for (;;) {
+        unsigned long long p = atomicAdd(queue, 1ull);
+        if (p >= N) break;
+        trace_photon<DEPTH>(P, (long long)p, props, flags, A, L, latz, sl, tl);
+    }
+    // warp reduction of the per-thread channels
+    double v0 = tl.absorbed, v1 = tl.absorbed_void, v2 = tl.gain;
+    unsigned long long c0 = tl.collisions, c1 = tl.crossings, c2 = tl.reflections;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v0 += __shfl_xor_sync(0xffffffffu, v0, o);
+        v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+        v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+        c0 += __shfl_xor_sync(0xffffffffu, c0, o);
+        c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+        c2 += __shfl_xor_sync(0xffffffffu, c2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&sl[BD_LEDGER_ABSORBED], v0);
+        atomicAdd(&sl[BD_LEDGER_ABSORBED_VOID], v1);
+        atomicAdd(&sl[BD_LEDGER_ROULETTE_GAIN], v2);
+        atomicAdd(&sl[BD_LEDGER_COLLISIONS], (double)c0);
+        atomicAdd(&sl[BD_LEDGER_CROSSINGS], (double)c1);
+        atomicAdd(&sl[BD_LEDGER_REFLECTIONS], (double)c2);
+    }
+    __syncthreads();
+    if (threadIdx.x < BD_LEDGER_LEN) partials[(size_t)blockIdx.x * BD_LEDGER_LEN + threadIdx.x] = sl[threadIdx.x];
+}
+
+// Fixed-order reduction of the per-block partials (deterministic for a given grid).
+__global__ void k_ledger_reduce(const double* __restrict__ partials, int nblocks, double launched,
+                                double* __restrict__ ledger) {
+    int ch = threadIdx.x;
+    if (ch >= BD_LEDGER_LEN) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partials[(size_t)b * BD_LEDGER_LEN + ch];
+    if (ch == BD_LEDGER_LAUNCHED) s = launched;
+    ledger[ch] = s;
+}
+
+__global__ void k_pack_props(const float* __restrict__ mu_a, const float* __restrict__ mu_s,
+                             const float* __restrict__ g, const float* __restrict__ n,
+                             const float* __restrict__ mu_ext, const uint8_t* __restrict__ flags,
+                             float ra, float rs, float g_plume, long long nv, float4* __restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv;
+         i += (long long)gridDim.x * blockDim.x) {
+        float a = mu_a[i], s = mu_s[i], gg = g[i], nn = n[i];
+        if (mu_ext != nullptr) {
+            float e = mu_ext[i];
+            a = a + e * ra;
+            s = s + e * rs;
+            if (e > 0.001f && (flags[i] & BD_FLAG_ABLATED)) gg = g_plume;
+        }
+        float mt = a + s;
+        float ratio = mt > 0.0f ? a / mt : 0.0f;
+        out[i] = make_float4(mt, ratio, gg, nn);
+    }
+}
+
+__global__ void k_fold(float* __restrict__ src, double* __restrict__ dst, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        float v = src[i];
+        if (v != 0.0f) {
+            dst[i] += (double)v;
+            src[i] = 0.0f;
+        }
+    }
+}
+
+}  // namespace bd
+
+// ------------------------------------------------------------------------------------
+struct BdMcContext {
+    unsigned long long* queue = nullptr;
+    double* partials = nullptr;
+    int partial_blocks = 0;
+    int device = -1;
+    int sm_count = 148;
+};
+
+using namespace bd;
+
+extern "C" int bd_mc_create(BdMcContext** out) {
+    BD_REQUIRE(out != nullptr, "bd_mc_create: out is NULL");
+    BdMcContext* c = new BdMcContext();
+    BD_CUDA(cudaGetDevice(&c->device));
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
+    // 16 resident 128-thread blocks per SM is the occupancy ceiling of k_mc_trace
+    c->partial_blocks = c->sm_count * 16;
+    cudaError_t e = cudaMalloc(&c->queue, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&c->partials, sizeof(double) * BD_LEDGER_LEN * c->partial_blocks);
+    if (e != cudaSuccess) {
+        cudaFree(c->queue);
+        delete c;
+        return cuda_status(e, "bd_mc_create: cudaMalloc");
+    }
+    *out = c;
+    return BD_OK;
+}
+
+extern "C" int bd_mc_destroy(BdMcContext* c) {
+    if (!c) return BD_OK;
+    cudaFree(c->queue);
+    cudaFree(c->partials);
+    delete c;
+    return BD_OK;
+}
+
+namespace bd {
+int mc_validate(const BdMcParams* p) {
+    BD_REQUIRE(p != nullptr, "bd_mc_trace: params is NULL");
+    BD_REQUIRE(p->nx > 0 && p->ny > 0 && p->nz > 0, "bd_mc_trace: grid dims must be positive");
+    BD_REQUIRE(p->dx > 0 && p->dy > 0 && p->dz > 0, "bd_mc_trace: voxel size must be positive");
+    BD_REQUIRE(p->launch_axis == 0 || p->launch_axis == 1, "bd_mc_trace: launch_axis must be 0 (z) or 1 (x)");
+    BD_REQUIRE(p->beam_profile >= 0 && p->beam_profile <= 3, "bd_mc_trace: unknown beam profile %d", p->beam_profile);
+    BD_REQUIRE(p->n_photons >= 0, "bd_mc_trace: n_photons must be >= 0");
+    BD_REQUIRE(p->max_events > 0, "bd_mc_trace: max_events must be > 0");
+    BD_REQUIRE(p->cos_th_safe > 0.0f, "bd_mc_trace: cos_th_safe must be > 0");
+    return BD_OK;
+}
+
+McDev mc_dev_params(const BdMcParams* p) {
+    McDev d;
+    d.nx = p->nx; d.ny = p->ny; d.nz = p->nz; d.launch_axis = p->launch_axis;
+    d.dx = p->dx; d.dy = p->dy; d.dz = p->dz; d.lx = p->lx; d.ly = p->ly; d.lz = p->lz;
+    d.ux0 = p->init_ux; d.uy0 = p->init_uy; d.uz0 = p->init_uz;
+    d.cos_ph = p->cos_ph; d.sin_ph = p->sin_ph; d.cos_th_safe = p->cos_th_safe;
+    d.xc = p->x_center; d.yc = p->y_center; d.zc = p->z_center;
+    d.sigma = p->sigma_axis; d.radius = p->beam_radius; d.profile = p->beam_profile;
+    d.n_amb = p->n_ambient; d.rmax2 = p->r_max_sq; d.options = p->options;
+    d.n_photons = p->n_photons; d.offset = p->photon_offset; d.max_events = p->max_events;
+    d.seed = p->seed;
+    const bool metal = (p->options & BD_MC_METAL_SEMANTICS) != 0;
+    d.eq_eps = metal ? 1e-6f : 1e-9f;
+    d.step_eps = metal ? 1e-4f : 1e-9f;
+    d.entry_eps = metal ? 1e-6f : 1e-9f;
+    return d;
+}
+
+// Launch with caller-provided scratch (queue counter + per-block partials).
+int mc_launch(const BdMcParams* p, const float* props, const uint8_t* flags, float* A, float* L,
+              double* latz, double* ledger, unsigned long long* queue, double* partials, int max_blocks,
+              int sm_count, cudaStream_t st) {
+    McDev d = mc_dev_params(p);
+    int blocks = (int)std::min<long long>((p->n_photons + 127) / 128, (long long)sm_count * 16);
+    blocks = std::max(1, std::min(blocks, max_blocks));
+    BD_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st));
+    const float4* pr = reinterpret_cast<const float4*>(props);
+    if (p->launch_axis == 0)
+        k_mc_trace<2><<<blocks, 128, 0, st>>>(d, pr, flags, A, L, latz, queue, partials);
+    else
+        k_mc_trace<0><<<blocks, 128, 0, st>>>(d, pr, flags, A, L, latz, queue, partials);
+    BD_CHECK_LAUNCH("k_mc_trace");
+    k_ledger_reduce<<<1, 32, 0, st>>>(partials, blocks, (double)p->n_photons, ledger);
+    BD_CHECK_LAUNCH("k_ledger_reduce");
+    return BD_OK;
+}
+}  // namespace bd
+
+extern "C" int bd_mc_trace(BdMcContext* c, const BdMcParams* p, const float* props, const uint8_t* flags,
+                           float* A, float* L, double* lat_depth, double* ledger, void* stream) {
+    BD_REQUIRE(c != nullptr, "bd_mc_trace: context is NULL");
+    int rc = mc_validate(p);
+    if (rc) return rc;
+    BD_REQUIRE(props != nullptr && A != nullptr && ledger != nullptr, "bd_mc_trace: props, A and ledger are required");
+    BD_REQUIRE(!(p->options & BD_MC_TALLY_FLUENCE) || L != nullptr, "bd_mc_trace: BD_MC_TALLY_FLUENCE needs L");
+    return mc_launch(p, props, flags, A, L, lat_depth, ledger, c->queue, c->partials, c->partial_blocks,
+                     c->sm_count, as_stream(stream));
+}
+
+extern "C" int bd_mc_pack_props(const float* mu_a, const float* mu_s, const float* g, const float* n,
+                                const float* mu_ext, const uint8_t* flags, float ra, float rs, float g_plume,
+                                int64_t nv, float* out, void* stream) {
+    BD_REQUIRE(mu_a && mu_s && g && n && out, "bd_mc_pack_props: NULL property pointer");
+    BD_REQUIRE(nv >= 0, "bd_mc_pack_props: negative size");
+    BD_REQUIRE(mu_ext == nullptr || flags != nullptr, "bd_mc_pack_props: plume extinction needs flags");
+    if (nv == 0) return BD_OK;
+    k_pack_props<<<grid_for(nv, 256), 256, 0, as_stream(stream)>>>(mu_a, mu_s, g, n, mu_ext, flags, ra, rs,
+                                                                    g_plume, nv, reinterpret_cast<float4*>(out));
+    BD_CHECK_LAUNCH("k_pack_props");
+    return BD_OK;
+}
+
+extern "C" int bd_fold_f32_to_f64(float* src, double* dst, int64_t n, void* stream) {
+    BD_REQUIRE(src && dst, "bd_fold_f32_to_f64: NULL pointer");
+    if (n <= 0) return BD_OK;
+    k_fold<<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(src, dst, n);
+    BD_CHECK_LAUNCH("k_fold");
+    return BD_OK;
+}

@@ -1,0 +1,362 @@
+// Explicit 7-point bioheat stencil, fused ablation substep and plume transport.
+//
+// Thermal update (voxel_thermal_3d.py:30-112, voxel_thermal_metal.py:56-134):
+//   T' = T + dt (sum_faces k_face (T_nb - T) / d^2 + Q) / rho_cp,
+//   k_face = 2 k_c k_n / (k_c + k_n + 1e-12); x/y faces insulated; z faces convective
+//   (series half-cell + h_eff, or the Metal fused kernel's -h_eff (T - T_amb)/dz).
+// Fused substep (metal_ablation_solver.py:71-191; CPU twin coupled_ablation.py:515-531):
+//   + latent-heat plateau (voxel_thermal_3d.py:115-143), Arrhenius damage
+//   (coupled_ablation.py:33-40) and first-order char kinetics (coupled_ablation.py:43-58),
+//   all pointwise on the trial temperature, so one pass per substep does everything.
+// Plume (plume.py:18-80, metal_ablation_solver.py:193-240): FTCS diffusion + upwind drift
+//   in the void domain, Neumann at solid walls, Dirichlet 0 on the outer walls.
+//
+// Layout: z fastest. A CTA owns a 32 (z) x 8 (y) column tile and marches along x (the
+// slowest axis), rotating the x-1 / x / x+1 values of T and k through registers, so each
+// T and k value is fetched from DRAM once per substep; y/z neighbours come from L1.
+#include "common.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace bd {
+
+constexpr int TZ = 32, TY = 8;
+
+struct Geo {
+    int nx, ny, nz, ni;
+    float idx2, idy2, idz2, dz, h_eff, t_amb, dt;
+};
+
+__device__ __forceinline__ float kface(float a, float b) { return 2.0f * a * b / (a + b + 1e-12f); }
+
+template <int BC>
+__device__ __forceinline__ float zwall_flux(float Tc, float kc, const Geo& g) {
+    if (BC == BD_BC_SERIES) {
+        // voxel_thermal_3d.py:97,105
+        return g.h_eff > 0.0f
+                   ? (g.t_amb - Tc) / (g.dz * (0.5f * g.dz / fmaxf(kc, 1e-30f) + 1.0f / fmaxf(g.h_eff, 1e-30f)))
+                   : 0.0f;
+    } else {
+        // metal_ablation_solver.py:141,150
+        return -g.h_eff * (Tc - g.t_amb) / g.dz;
+    }
+}
+
+struct AblConst {
+    float t_abl, t_void, q_scale;
+    float arr_A, arr_EaR, char_A, char_EaR;
+    int zero_src_in_ablated, is_active;
+};
+
+// MODE 0: thermal only. MODE 1: fused ablation substep.
+template <int MODE, int BC, bool ARR, bool CHAR>
+__global__ void __launch_bounds__(TZ * TY) k_substep(Geo g, AblConst c, const float* __restrict__ T,
+                                                     float* __restrict__ Tn, const float* __restrict__ src,
+                                                     const float* __restrict__ K, const float* __restrict__ R,
+                                                     const uint8_t* __restrict__ F, float* __restrict__ H,
+                                                     float* __restrict__ Om, float* __restrict__ Chi) {
+    const int k = blockIdx.x * TZ + threadIdx.x;
+    const int j = blockIdx.y * TY + threadIdx.y;
+    if (k >= g.nz || j >= g.ny) return;
+    const int i0 = blockIdx.z * g.ni;
+    const int i1 = min(i0 + g.ni, g.nx);
+    const size_t plane = (size_t)g.ny * g.nz;
+    const size_t base = (size_t)j * g.nz + k;
+
+    float Tm = 0.0f, km = 0.0f;
+    size_t idx = (size_t)i0 * plane + base;
+    float Tc = __ldg(&T[idx]), kc = __ldg(&K[idx]);
+    if (i0 > 0) { Tm = __ldg(&T[idx - plane]); km = __ldg(&K[idx - plane]); }
+
+    for (int i = i0; i < i1; ++i, idx += plane) {
+        float Tp = 0.0f, kp = 0.0f;
+        const bool has_e = (i + 1 < g.nx);
+        if (has_e) { Tp = __ldg(&T[idx + plane]); kp = __ldg(&K[idx + plane]); }
+
+        float fw = (i > 0) ? kface(kc, km) * (Tm - Tc) * g.idx2 : 0.0f;
+        float fe = has_e ? kface(kc, kp) * (Tp - Tc) * g.idx2 : 0.0f;
+        float fs = 0.0f, fn = 0.0f, ft, fb;
+        if (j > 0)        fs = kface(kc, __ldg(&K[idx - g.nz])) * (__ldg(&T[idx - g.nz]) - Tc) * g.idy2;
+        if (j + 1 < g.ny) fn = kface(kc, __ldg(&K[idx + g.nz])) * (__ldg(&T[idx + g.nz]) - Tc) * g.idy2;
+        if (k > 0)        ft = kface(kc, __ldg(&K[idx - 1])) * (__ldg(&T[idx - 1]) - Tc) * g.idz2;
+        else              ft = zwall_flux<BC>(Tc, kc, g);
+        if (k + 1 < g.nz) fb = kface(kc, __ldg(&K[idx + 1])) * (__ldg(&T[idx + 1]) - Tc) * g.idz2;
+        else              fb = zwall_flux<BC>(Tc, kc, g);
+        const float div = fw + fe + fs + fn + ft + fb;
+
+        const float rho = __ldg(&R[idx]);
+        const float cap = fmaxf(rho, 1e-12f);
+        uint8_t f = 0;
+        if (MODE == 1) f = __ldg(&F[idx]);
+        float q = 0.0f;
+        if (c.is_active) {
+            q = __ldg(&src[idx]) * c.q_scale;
+            if (MODE == 1 && c.zero_src_in_ablated && (f & BD_FLAG_ABLATED)) q = 0.0f;
+        }
+        float Tt = Tc + g.dt * (div + q) / cap;
+
+        if (MODE == 1) {
+            const bool abl = (f & BD_FLAG_ABLATED) != 0;
+            const bool dry = (f & BD_FLAG_DRY) != 0;
+            if (abl) {
+                if (Tt > c.t_void) Tt = c.t_void;
+            } else if (!dry) {
+                float h = H[idx];
+                if (Tt > c.t_abl) {
+                    h += (Tt - c.t_abl) * rho;
+                    Tt = c.t_abl;
+                    H[idx] = h;
+                } else if (h > 0.0f) {
+                    float rel = fminf(h, (c.t_abl - Tt) * rho);
+                    H[idx] = h - rel;
+                    Tt = Tt + rel / rho;
+                }
+            }
+            if (ARR && !abl) Om[idx] += g.dt * c.arr_A * expf(-c.arr_EaR / (Tt + 273.15f));
+            if (CHAR && dry && !abl) {
+                float rate = c.char_A * expf(-c.char_EaR / (Tt + 273.15f));
+                float x = Chi[idx];
+                Chi[idx] = 1.0f - (1.0f - x) * expf(-rate * g.dt);
+            }
+        }
+        Tn[idx] = Tt;
+        Tm = Tc; km = kc; Tc = Tp; kc = kp;
+    }
+}
+
+struct PlumeConst {
+    float dxy_x, dxy_y, dz_z;  // D_xy*idx2, D_xy*idy2, D_z*idz2
+    float vz_over_dz, dtp, decay;
+};
+
+// One FTCS plume step over the whole grid (plume.py:46-80).
+__global__ void __launch_bounds__(TZ * TY) k_plume_step(int nx, int ny, int nz, int ni, PlumeConst c,
+                                                        const float* __restrict__ C, float* __restrict__ Cn,
+                                                        const uint8_t* __restrict__ F) {
+    const int k = blockIdx.x * TZ + threadIdx.x;
+    const int j = blockIdx.y * TY + threadIdx.y;
+    if (k >= nz || j >= ny) return;
+    const int i0 = blockIdx.z * ni;
+    const int i1 = min(i0 + ni, nx);
+    const size_t plane = (size_t)ny * nz;
+    size_t idx = (size_t)i0 * plane + (size_t)j * nz + k;
+    const bool jk_wall = (j == 0 || j == ny - 1 || k == 0 || k == nz - 1);
+    for (int i = i0; i < i1; ++i, idx += plane) {
+        const uint8_t f = __ldg(&F[idx]);
+        if (!(f & BD_FLAG_VOID) || jk_wall || i == 0 || i == nx - 1) {
+            Cn[idx] = 0.0f;
+            continue;
+        }
+        const float cc = __ldg(&C[idx]);
+        const float cw = (__ldg(&F[idx - plane]) & BD_FLAG_VOID) ? __ldg(&C[idx - plane]) : cc;
+        const float ce = (__ldg(&F[idx + plane]) & BD_FLAG_VOID) ? __ldg(&C[idx + plane]) : cc;
+        const float cs = (__ldg(&F[idx - nz]) & BD_FLAG_VOID) ? __ldg(&C[idx - nz]) : cc;
+        const float cn = (__ldg(&F[idx + nz]) & BD_FLAG_VOID) ? __ldg(&C[idx + nz]) : cc;
+        const float cb = (__ldg(&F[idx - 1]) & BD_FLAG_VOID) ? __ldg(&C[idx - 1]) : cc;
+        const float ct = (__ldg(&F[idx + 1]) & BD_FLAG_VOID) ? __ldg(&C[idx + 1]) : cc;
+        const float diff = c.dxy_x * (cw - 2.0f * cc + ce) + c.dxy_y * (cs - 2.0f * cc + cn) +
+                           c.dz_z * (cb - 2.0f * cc + ct);
+        const float adv = -c.vz_over_dz * (cc - ct);
+        const float v = (cc + c.dtp * (diff + adv)) * c.decay;
+        Cn[idx] = fmaxf(v, 0.0f);
+    }
+}
+
+__global__ void k_pack_flags(const uint8_t* __restrict__ abl, const uint8_t* __restrict__ dry,
+                             const uint8_t* __restrict__ vd, long long n, uint8_t* __restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        uint8_t a = abl[i] ? 1 : 0, d = dry[i] ? 1 : 0;
+        uint8_t v = vd ? (vd[i] ? 1 : 0) : a;
+        out[i] = (uint8_t)(a * BD_FLAG_ABLATED | d * BD_FLAG_DRY | v * BD_FLAG_VOID);
+    }
+}
+
+static dim3 tile_grid(int nx, int ny, int nz, int ni) {
+    return dim3((nz + TZ - 1) / TZ, (ny + TY - 1) / TY, (nx + ni - 1) / ni);
+}
+
+static int pick_ni(int nx, int ny, int nz) {
+    // aim for ~8 resident CTAs of 256 threads on each of 148 SMs
+    long long cols = (long long)((nz + TZ - 1) / TZ) * ((ny + TY - 1) / TY);
+    long long want = 148LL * 8;
+    long long chunks = std::max(1LL, want / std::max(1LL, cols));
+    int ni = (int)std::max(4LL, ((long long)nx + chunks - 1) / chunks);
+    return std::min(ni, std::max(nx, 1));
+}
+
+static Geo make_geo(int nx, int ny, int nz, float dx, float dy, float dz, float dt, float h, float tamb) {
+    Geo g;
+    g.nx = nx; g.ny = ny; g.nz = nz;
+    g.ni = pick_ni(nx, ny, nz);
+    g.idx2 = 1.0f / (dx * dx); g.idy2 = 1.0f / (dy * dy); g.idz2 = 1.0f / (dz * dz);
+    g.dz = dz; g.h_eff = h; g.t_amb = tamb; g.dt = dt;
+    return g;
+}
+
+template <int MODE, int BC, bool ARR, bool CHAR>
+static void launch_substeps(const Geo& g, const AblConst& c, float* Ta, float* Tb, int n, const float* src,
+                            const float* K, const float* R, const uint8_t* F, float* H, float* Om, float* Chi,
+                            cudaStream_t st) {
+    dim3 grid = tile_grid(g.nx, g.ny, g.nz, g.ni), block(TZ, TY);
+    for (int s = 0; s < n; ++s) {
+        const float* in = (s & 1) ? Tb : Ta;
+        float* out = (s & 1) ? Ta : Tb;
+        k_substep<MODE, BC, ARR, CHAR><<<grid, block, 0, st>>>(g, c, in, out, src, K, R, F, H, Om, Chi);
+    }
+}
+
+int plume_policy_steps(const BdPlumeParams* p, int* n_steps, float* dt_step, float* decay_step) {
+    const double idx2 = 1.0 / ((double)p->dx * p->dx), idy2 = 1.0 / ((double)p->dy * p->dy);
+    const double idz2 = 1.0 / ((double)p->dz * p->dz);
+    const double d_rate = (double)p->D_xy * (idx2 + idy2) + (double)p->D_z * idz2;
+    const double dt = p->dt;
+    const bool decays = p->tau_linger > 0.0f && std::isfinite(p->tau_linger);
+    if (p->dt_policy == BD_PLUME_DT_AS_GIVEN) {
+        *n_steps = 1; *dt_step = (float)dt;
+        *decay_step = decays ? (float)std::exp(-dt / p->tau_linger) : 1.0f;
+    } else if (p->dt_policy == BD_PLUME_DT_METAL) {
+        // dt_plume = min(dt, 0.45 / (2 d_rate)); decay still uses the substep dt
+        float dr = (float)p->D_xy * ((float)idx2 + (float)idy2) + (float)p->D_z * (float)idz2;
+        *n_steps = 1;
+        *dt_step = dr > 1e-6f ? std::min((float)dt, 0.45f / (2.0f * dr)) : (float)dt;
+        *decay_step = decays ? (float)std::exp(-dt / p->tau_linger) : 1.0f;
+    } else if (p->dt_policy == BD_PLUME_DT_SUBCYCLE) {
+        int n = p->n_sub;
+        if (n <= 0) {
+            // FTCS with upwind drift keeps every coefficient >= 0 while
+            // dt (2 d_rate + vz/dz) <= 1; use 90 % of that limit.
+            const double rate = 2.0 * d_rate + std::max(0.0, (double)p->vz) / p->dz;
+            n = std::max(1, (int)std::ceil(dt * rate / 0.9 - 1e-9));
+        }
+        *n_steps = n;
+        *dt_step = (float)(dt / n);
+        *decay_step = decays ? (float)std::exp(-(dt / n) / p->tau_linger) : 1.0f;
+    } else {
+        return fail(BD_ERR_INVALID_ARG, "unknown plume dt policy %d", p->dt_policy);
+    }
+    return BD_OK;
+}
+
+}  // namespace bd
+
+using namespace bd;
+
+extern "C" int bd_thermal_advance(const BdThermalParams* p, float* Ta, float* Tb, int n, const float* src,
+                                  const float* K, const float* R, void* stream) {
+    BD_REQUIRE(p != nullptr, "bd_thermal_advance: params is NULL");
+    BD_REQUIRE(p->nx > 0 && p->ny > 0 && p->nz > 0, "bd_thermal_advance: grid dims must be positive");
+    BD_REQUIRE(Ta && Tb && K && R, "bd_thermal_advance: NULL field");
+    BD_REQUIRE(!p->is_active || src != nullptr, "bd_thermal_advance: active source needs src");
+    BD_REQUIRE(p->bc_mode == BD_BC_SERIES || p->bc_mode == BD_BC_METAL, "bd_thermal_advance: bad bc_mode");
+    BD_REQUIRE(n >= 0, "bd_thermal_advance: n_substeps must be >= 0");
+    if (n == 0) return BD_OK;
+    Geo g = make_geo(p->nx, p->ny, p->nz, p->dx, p->dy, p->dz, p->dt, p->h_eff, p->t_ambient);
+    AblConst c{};
+    c.q_scale = p->q_scale;
+    c.is_active = p->is_active;
+    cudaStream_t st = as_stream(stream);
+    if (p->bc_mode == BD_BC_SERIES)
+        launch_substeps<0, BD_BC_SERIES, false, false>(g, c, Ta, Tb, n, src, K, R, nullptr, nullptr, nullptr, nullptr, st);
+    else
+        launch_substeps<0, BD_BC_METAL, false, false>(g, c, Ta, Tb, n, src, K, R, nullptr, nullptr, nullptr, nullptr, st);
+    BD_CHECK_LAUNCH("k_substep<thermal>");
+    return BD_OK;
+}
+
+namespace bd {
+int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, float* H, float* Om, float* Chi,
+                    const uint8_t* F, const float* src, const float* K, const float* R, cudaStream_t st) {
+    Geo g = make_geo(p->nx, p->ny, p->nz, p->dx, p->dy, p->dz, p->dt, p->h_eff, p->t_ambient);
+    AblConst c;
+    c.t_abl = p->t_abl; c.t_void = p->t_void; c.q_scale = p->q_scale;
+    c.arr_A = p->arr_A; c.arr_EaR = p->arr_Ea_over_R; c.char_A = p->char_A; c.char_EaR = p->char_Ea_over_R;
+    c.zero_src_in_ablated = p->zero_src_in_ablated; c.is_active = p->is_active;
+    const bool arr = p->has_arrhenius != 0, chr = p->has_char != 0;
+#define BD_ABL_CASE(BCV, A_, C_)                                                                 \
+    if (p->bc_mode == BCV && arr == A_ && chr == C_) {                                           \
+        launch_substeps<1, BCV, A_, C_>(g, c, Ta, Tb, n, src, K, R, F, H, Om, Chi, st);          \
+        BD_CHECK_LAUNCH("k_substep<ablation>");                                                  \
+        return BD_OK;                                                                            \
+    }
+    BD_ABL_CASE(BD_BC_SERIES, false, false)
+    BD_ABL_CASE(BD_BC_SERIES, false, true)
+    BD_ABL_CASE(BD_BC_SERIES, true, false)
+    BD_ABL_CASE(BD_BC_SERIES, true, true)
+    BD_ABL_CASE(BD_BC_METAL, false, false)
+    BD_ABL_CASE(BD_BC_METAL, false, true)
+    BD_ABL_CASE(BD_BC_METAL, true, false)
+    BD_ABL_CASE(BD_BC_METAL, true, true)
+#undef BD_ABL_CASE
+    return fail(BD_ERR_INVALID_ARG, "bd_ablation_advance: bad bc_mode %d", p->bc_mode);
+}
+
+int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
+                 cudaStream_t st) {
+    int steps;
+    float dtp, decay;
+    int rc = plume_policy_steps(p, &steps, &dtp, &decay);
+    if (rc) return rc;
+    PlumeConst c;
+    c.dxy_x = p->D_xy / (p->dx * p->dx);
+    c.dxy_y = p->D_xy / (p->dy * p->dy);
+    c.dz_z = p->D_z / (p->dz * p->dz);
+    c.vz_over_dz = p->vz > 0.0f ? p->vz / p->dz : 0.0f;
+    c.dtp = dtp;
+    c.decay = decay;
+    const int ni = pick_ni(p->nx, p->ny, p->nz);
+    dim3 grid = tile_grid(p->nx, p->ny, p->nz, ni), block(TZ, TY);
+    const long long total = (long long)steps * n_substeps;
+    for (long long s = 0; s < total; ++s) {
+        const float* in = (s & 1) ? Cb : Ca;
+        float* out = (s & 1) ? Ca : Cb;
+        k_plume_step<<<grid, block, 0, st>>>(p->nx, p->ny, p->nz, ni, c, in, out, F);
+    }
+    BD_CHECK_LAUNCH("k_plume_step");
+    if (in_b) *in_b = (int)(total & 1);
+    return BD_OK;
+}
+}  // namespace bd
+
+extern "C" int bd_ablation_advance(const BdAblationParams* p, float* Ta, float* Tb, int n, float* H, float* Om,
+                                   float* Chi, const uint8_t* F, const float* src, const float* K, const float* R,
+                                   void* stream) {
+    BD_REQUIRE(p != nullptr, "bd_ablation_advance: params is NULL");
+    BD_REQUIRE(p->nx > 0 && p->ny > 0 && p->nz > 0, "bd_ablation_advance: grid dims must be positive");
+    BD_REQUIRE(Ta && Tb && H && F && K && R, "bd_ablation_advance: NULL field");
+    BD_REQUIRE(!p->is_active || src != nullptr, "bd_ablation_advance: active source needs src");
+    BD_REQUIRE(!p->has_arrhenius || Om != nullptr, "bd_ablation_advance: Arrhenius needs Omega");
+    BD_REQUIRE(!p->has_char || Chi != nullptr, "bd_ablation_advance: char kinetics need chi");
+    BD_REQUIRE(n >= 0, "bd_ablation_advance: n_substeps must be >= 0");
+    if (n == 0) return BD_OK;
+    return ablation_launch(p, Ta, Tb, n, H, Om, Chi, F, src, K, R, as_stream(stream));
+}
+
+extern "C" int bd_plume_advance(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F,
+                                int* in_b, void* stream) {
+    BD_REQUIRE(p != nullptr, "bd_plume_advance: params is NULL");
+    BD_REQUIRE(p->nx > 0 && p->ny > 0 && p->nz > 0, "bd_plume_advance: grid dims must be positive");
+    BD_REQUIRE(Ca && Cb && F, "bd_plume_advance: NULL field");
+    BD_REQUIRE(n_substeps >= 0, "bd_plume_advance: n_substeps must be >= 0");
+    if (n_substeps == 0) {
+        if (in_b) *in_b = 0;
+        return BD_OK;
+    }
+    return plume_launch(p, Ca, Cb, n_substeps, F, in_b, as_stream(stream));
+}
+
+extern "C" int bd_plume_steps_per_substep(const BdPlumeParams* p, int* n_steps, float* dt_step) {
+    BD_REQUIRE(p && n_steps && dt_step, "bd_plume_steps_per_substep: NULL argument");
+    float decay;
+    return plume_policy_steps(p, n_steps, dt_step, &decay);
+}
+
+extern "C" int bd_pack_flags(const uint8_t* abl, const uint8_t* dry, const uint8_t* vd, int64_t n, uint8_t* out,
+                             void* stream) {
+    BD_REQUIRE(abl && dry && out, "bd_pack_flags: NULL mask");
+    if (n <= 0) return BD_OK;
+    k_pack_flags<<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(abl, dry, vd, n, out);
+    BD_CHECK_LAUNCH("k_pack_flags");
+    return BD_OK;
+}
