@@ -163,6 +163,7 @@ def run_ours(args, rank, world, local):
     for _ in range(W):
         eng.power = POWER_W
         eng._enqueue(0)
+    laser_diag = eng._diag(None) if W > 0 else None
     torch.cuda.synchronize()
     lib = _lib.load()
     lib.bd_engine_timing(eng._handle, 1)
@@ -192,7 +193,7 @@ def run_ours(args, rank, world, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     res = {"ms": ms, "K": K, "n_on": n_on, "stage_ms": stage_ms, "clocks": clk.summary(), "eng": eng, "geo": geo,
-           "last_diag": d}
+           "last_diag": d, "laser_diag": laser_diag}
     return res
 
 
@@ -282,6 +283,15 @@ def ours_main(args):
     photons = r["n_on"] * eng.n_photons
     mc = {"photons_per_s": photons / (mc_ms * 1e-3) if mc_ms > 0 else None,
           "mc_ms_per_laser_epoch": mc_ms / max(r["n_on"], 1)}
+    if r["laser_diag"] is not None:
+        from bug_defense_b200 import _lib as L_
+        ld = r["laser_diag"]["ledger"]
+        steps_per_epoch = float(ld[L_.LEDGER_COLLISIONS] + ld[L_.LEDGER_CROSSINGS])
+        mc["photon_steps_per_laser_epoch"] = steps_per_epoch
+        if mc_ms > 0:
+            mc["photon_steps_per_s"] = steps_per_epoch * r["n_on"] / (mc_ms * 1e-3)
+        lc = (ld[1:7].sum() + ld[8] + ld[9] - ld[7]) / max(ld[0], 1)
+        mc["ledger_closure_minus_1"] = float(lc - 1.0)
     gpu_launches = K * (1 + 3 + eng.n_substeps + eng.n_substeps * n_plume_sub) + r["n_on"] * 2
     out = {"metric": METRIC, "value": round(value, 3), "unit": "epochs/s", "n_gpus": world, "steps": K,
            "warmup": args.warmup, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",

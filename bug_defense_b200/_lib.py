@@ -100,6 +100,7 @@ class PlumeParams(Structure):
 
 FLAG_NEWLY = 0x08
 EPOCH_SKIP_MC = 0x1
+EPOCH_NO_GRAPH = 0x2
 
 
 class GridRef(Structure):

@@ -16,6 +16,7 @@ Extensions (keywords the reference does not have):
   bc               'series' (voxel_thermal_3d.py:97,105) or 'metal' (metal_ablation_solver.py:141,150)
   semantics        'cpu' or 'metal' deltas of the photon tracer
   tally_fluence    also tally the track-length estimator for Phi
+  use_graphs       replay each epoch stage as a captured CUDA graph (default) or launch directly
 """
 from __future__ import annotations
 
@@ -73,7 +74,7 @@ class CoupledAblationEngine:
                  initial_dry_mask=None, initial_ablated_mask=None, air_gap_range=None,
                  wavelength_nm: float = 10600.0, mc_engine: str = 'auto', thermal_engine: str = 'auto',
                  seed=None, plume_dt_policy: str = 'subcycle', bc: str = 'series', semantics: str = 'cpu',
-                 tally_fluence: bool = True, device=None):
+                 tally_fluence: bool = True, use_graphs: bool = True, device=None):
         for name, eng in (('mc_engine', mc_engine), ('thermal_engine', thermal_engine)):
             e = str(eng).strip().lower()
             if e == 'cpu':
@@ -103,6 +104,7 @@ class CoupledAblationEngine:
         self.theta_inc_deg, self.phi_inc_deg = float(theta_inc_deg), float(phi_inc_deg)
         self.semantics = semantics
         self.tally_fluence = bool(tally_fluence)
+        self.use_graphs = bool(use_graphs)
         self.seed = int(seed) if seed is not None else int(np.random.randint(1, 2 ** 31 - 1))
 
         k = np.array(k_grid, dtype=np.float64, copy=True)
@@ -297,27 +299,8 @@ class CoupledAblationEngine:
                            seed=self.seed, semantics=self.semantics, tally_fluence=self.tally_fluence)
 
     def _init_flags_and_props(self):
+        # bd_engine_create already ran the initial void / plume / packed-property pass
         _lib.call("bd_engine_set_time", self._handle, 0.0, 0, _lib.stream_ptr())
-        # the epoch-end pass without removal work: nothing is removed (apply on a copy of the
-        # phase state would change properties), so only the void / plume / props pass runs.
-        # The reference packs properties at the start of each epoch; the same values result.
-        self._pack_props_only()
-
-    def _pack_props_only(self):
-        pl = self.plume
-        ratio_a = pl.ratio_a if pl is not None else 0.0
-        ratio_s = pl.ratio_s if pl is not None else 0.0
-        _lib.call("bd_mc_pack_props", *(_lib.ptr(self._opt_t[key]) for key in ('mu_a', 'mu_s', 'g', 'n')),
-                  _lib.ptr(pl.mu_ext if pl is not None else None), _lib.ptr(self._flags if pl is not None else None),
-                  ratio_a, ratio_s, 0.80, self.Nx * self.Ny * self.Nz, _lib.ptr(self._props), _lib.stream_ptr())
-        # void bits for the plume domain of the first epoch (compute_void_mask at t = 0)
-        abl = (self._flags & _lib.FLAG_ABLATED) != 0
-        vd = abl.clone()
-        if self.air_gap_range is not None:
-            k0, k1 = self.air_gap_range
-            if k0 > 0 and bool(abl[:, :, k0 - 1].any()):
-                vd[:, :, k0:k1] = True
-        self._flags.copy_((self._flags & ~_lib.FLAG_VOID) | (vd.to(torch.uint8) * _lib.FLAG_VOID))
 
     # ------------------------------------------------------------------------------
     @property
@@ -349,12 +332,16 @@ class CoupledAblationEngine:
         voxel to use instead of running the MC this epoch (a fixed heat source)."""
         opts = 0
         if absorbed_map is not None:
-            self._A.copy_(to_dev(absorbed_map, self.dev).reshape(self.shape))
+            # the engine's tally holds absorbed weight for n_photons launched photons
+            tally = np.asarray(absorbed_map, dtype=np.float64) * max(self.n_photons, 1)
+            self._A.copy_(to_dev(tally, self.dev).reshape(self.shape))
             opts |= _lib.EPOCH_SKIP_MC
         self._enqueue(opts)
         return self._diag(absorbed_map)
 
     def _enqueue(self, opts=0):
+        if not self.use_graphs:
+            opts |= _lib.EPOCH_NO_GRAPH
         _lib.call("bd_engine_step_epoch", self._handle, float(self._power), int(opts), _lib.stream_ptr())
         self._last_power = self._power
 

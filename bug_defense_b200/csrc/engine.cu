@@ -10,10 +10,18 @@
 #include "engine.cuh"
 
 #include <algorithm>
+#include <cstring>
 #include <vector>
+
+struct StageGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<unsigned char> key;
+};
 
 struct BdEngine {
     BdEngineDesc d;
+    cudaStream_t cap_stream = nullptr;  // private stream used only to capture stage graphs
+    StageGraph g_mc, g_sub_on, g_sub_off, g_plume, g_end;
     bd::PhaseArgs pa;
     bd::EngineDyn* dyn = nullptr;      // device
     bd::EngineDyn* dyn_host = nullptr; // pinned
@@ -30,6 +38,41 @@ struct BdEngine {
     size_t ring_used = 0;
     int ring_error = 0;
 };
+
+static void graph_reset(StageGraph& g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+    g.key.clear();
+}
+
+// Launches `enqueue` as a captured graph on `st`, re-capturing when `key` changed.
+template <typename F>
+static int run_stage(BdEngine* e, StageGraph& g, const void* key, size_t key_len, bool use_graph, cudaStream_t st,
+                     F enqueue) {
+    if (!use_graph) return enqueue(st);
+    const unsigned char* kb = static_cast<const unsigned char*>(key);
+    if (!g.exec || g.key.size() != key_len || (key_len && memcmp(g.key.data(), kb, key_len) != 0)) {
+        graph_reset(g);
+        cudaGraph_t graph = nullptr;
+        BD_CUDA(cudaStreamBeginCapture(e->cap_stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue(e->cap_stream);
+        cudaError_t ce = cudaStreamEndCapture(e->cap_stream, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (ce != cudaSuccess) return bd::cuda_status(ce, "cudaStreamEndCapture");
+        ce = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) {
+            g.exec = nullptr;
+            return bd::cuda_status(ce, "cudaGraphInstantiate");
+        }
+        g.key.assign(kb, kb + key_len);
+    }
+    BD_CUDA(cudaGraphLaunch(g.exec, st));
+    return BD_OK;
+}
 
 static cudaEvent_t ring_event(BdEngine* e) {
     if (e->ring_used == e->ring.size()) {
@@ -128,6 +171,7 @@ static int validate(const BdEngineDesc* d) {
     BD_REQUIRE(!d->substep.has_char || p.chi, "bd_engine_create: char kinetics need chi");
     BD_REQUIRE(d->A != nullptr, "bd_engine_create: absorbed map A is required");
     BD_REQUIRE(d->voxel_volume > 0.0, "bd_engine_create: voxel_volume must be > 0");
+    BD_REQUIRE((long long)p.nx * p.ny * p.nz < (1LL << 31), "bd_engine_create: grid exceeds 2^31 voxels");
     return BD_OK;
 }
 
@@ -151,11 +195,23 @@ extern "C" int bd_engine_create(const BdEngineDesc* desc, BdEngine** out) {
     if (err == cudaSuccess) err = cudaMalloc(&e->partials, sizeof(double) * BD_LEDGER_LEN * e->partial_blocks);
     if (err == cudaSuccess) err = cudaMemset(e->dyn, 0, sizeof(EngineDyn));
     for (int q = 0; q < 4 && err == cudaSuccess; ++q) err = cudaEventCreate(&e->ev[q]);
+    if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->cap_stream, cudaStreamNonBlocking);
     if (err != cudaSuccess) {
         bd_engine_destroy(e);
         return cuda_status(err, "bd_engine_create");
     }
     e->pa = phase_args(desc->phase, e->dyn);
+    // initial void bits, gap state, plume extinction and packed MC properties for the first
+    // epoch (no removal: the reference changes no voxel before its first epoch end)
+    rc = phase_launch(e->pa, BD_PHASE_INIT, nullptr);
+    if (rc == BD_OK) {
+        err = cudaStreamSynchronize(nullptr);
+        if (err != cudaSuccess) rc = cuda_status(err, "bd_engine_create: initial pass");
+    }
+    if (rc) {
+        bd_engine_destroy(e);
+        return rc;
+    }
     *out = e;
     return BD_OK;
 }
@@ -169,6 +225,9 @@ extern "C" int bd_engine_destroy(BdEngine* e) {
     for (int q = 0; q < 4; ++q)
         if (e->ev[q]) cudaEventDestroy(e->ev[q]);
     for (cudaEvent_t ev : e->ring) cudaEventDestroy(ev);
+    graph_reset(e->g_mc); graph_reset(e->g_sub_on); graph_reset(e->g_sub_off);
+    graph_reset(e->g_plume); graph_reset(e->g_end);
+    if (e->cap_stream) cudaStreamDestroy(e->cap_stream);
     delete e;
     return BD_OK;
 }
@@ -177,6 +236,8 @@ extern "C" int bd_engine_set_time(BdEngine* e, double t, int64_t epoch, void* st
     BD_REQUIRE(e != nullptr, "bd_engine_set_time: NULL engine");
     k_set_time<<<1, 1, 0, as_stream(stream)>>>(e->dyn, t, (long long)epoch);
     e->epochs_enqueued = (long long)epoch;
+    // a graph-launched MC reads the photon offset from the device; keep it consistent
+
     BD_CHECK_LAUNCH("k_set_time");
     return BD_OK;
 }
@@ -187,51 +248,64 @@ extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void*
     cudaStream_t st = as_stream(stream);
     const BdEngineDesc& d = e->d;
     const long long nv = (long long)d.phase.nx * d.phase.ny * d.phase.nz;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    BD_CUDA(cudaStreamIsCapturing(st, &cap));
+    e->timed = (cap == cudaStreamCaptureStatusNone);
+    // stage graphs unless asked not to, or the caller is itself capturing into a graph
+    const bool graphs = !(options & BD_EPOCH_NO_GRAPH) && e->timed;
     k_epoch_begin<<<1, 32, 0, st>>>(e->dyn, d.dt_epoch);
     BD_CHECK_LAUNCH("k_epoch_begin");
-    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-    cudaStreamIsCapturing(st, &cap);
-    e->timed = (cap == cudaStreamCaptureStatusNone);
+    ++e->epochs_enqueued;
     mark(e, st, 0);
 
     const bool laser = power > 0.0f;
+    int rc = BD_OK;
     if (laser && !(options & BD_EPOCH_SKIP_MC)) {
         BD_REQUIRE(d.phase.props != nullptr, "bd_engine_step_epoch: MC needs the packed property buffer");
-        BD_CUDA(cudaMemsetAsync(d.A, 0, sizeof(float) * nv, st));
-        if (d.L && (d.mc.options & BD_MC_TALLY_FLUENCE)) BD_CUDA(cudaMemsetAsync(d.L, 0, sizeof(float) * nv, st));
         BdMcParams mp = d.mc;
-        // one 2^32 photon-index window per epoch keeps every epoch's Philox streams distinct
-        mp.photon_offset = (int64_t)(++e->epochs_enqueued) << 32;
-        int rc = mc_launch(&mp, d.phase.props, d.phase.flags, d.A, d.L, d.lat_depth, e->dyn->ledger, e->queue,
-                           e->partials, e->partial_blocks, e->sm_count, st);
+        mp.photon_offset = 0;  // the epoch's offset (epoch << 32) is read from device memory
+        rc = run_stage(e, e->g_mc, &mp, sizeof(mp), graphs, st, [&](cudaStream_t s) -> int {
+            BD_CUDA(cudaMemsetAsync(d.A, 0, sizeof(float) * nv, s));
+            if (d.L && (d.mc.options & BD_MC_TALLY_FLUENCE)) BD_CUDA(cudaMemsetAsync(d.L, 0, sizeof(float) * nv, s));
+            return mc_launch(&mp, d.phase.props, d.phase.flags, d.A, d.L, d.lat_depth, e->dyn->ledger, e->queue,
+                             e->partials, e->partial_blocks, e->sm_count, s, &e->dyn->mc_offset);
+        });
         if (rc) return rc;
-    } else {
-        ++e->epochs_enqueued;
     }
-
     mark(e, st, 1);
     if (d.n_substeps > 0) {
         BdAblationParams ap = d.substep;
         ap.is_active = laser ? 1 : 0;
-        ap.q_scale = (d.mc.n_photons > 0) ? (float)((double)power / ((double)d.mc.n_photons * d.voxel_volume)) : 0.0f;
+        ap.q_scale = (laser && d.mc.n_photons > 0)
+                         ? (float)((double)power / ((double)d.mc.n_photons * d.voxel_volume)) : 0.0f;
         ap.zero_src_in_ablated = 1;
-        int rc = ablation_launch(&ap, d.phase.T, d.T_alt, d.n_substeps, d.phase.H_acc, d.omega, d.phase.chi,
-                                 d.phase.flags, d.A, d.phase.k, d.phase.rho_cp, st);
+        rc = run_stage(e, laser ? e->g_sub_on : e->g_sub_off, &ap, sizeof(ap), graphs, st, [&](cudaStream_t s) -> int {
+            int r = ablation_launch(&ap, d.phase.T, d.T_alt, d.n_substeps, d.phase.H_acc, d.omega, d.phase.chi,
+                                    d.phase.flags, d.A, d.phase.k, d.phase.rho_cp, s);
+            if (r) return r;
+            if (d.n_substeps & 1)
+                BD_CUDA(cudaMemcpyAsync(d.phase.T, d.T_alt, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
+            return BD_OK;
+        });
         if (rc) return rc;
-        if (d.n_substeps & 1) BD_CUDA(cudaMemcpyAsync(d.phase.T, d.T_alt, sizeof(float) * nv, cudaMemcpyDeviceToDevice, st));
     }
     mark(e, st, -1);
-    if (d.n_substeps > 0) {
-        if (d.has_plume_transport) {
+    if (d.n_substeps > 0 && d.has_plume_transport) {
+        rc = run_stage(e, e->g_plume, &d.plume, sizeof(d.plume), graphs, st, [&](cudaStream_t s) -> int {
             int in_b = 0;
-            int rc = plume_launch(&d.plume, d.phase.plume, d.plume_alt, d.n_substeps, d.phase.flags, &in_b, st);
-            if (rc) return rc;
+            int r = plume_launch(&d.plume, d.phase.plume, d.plume_alt, d.n_substeps, d.phase.flags, &in_b, s,
+                                 &e->dyn->void_zlimit, 0);
+            if (r) return r;
             if (in_b)
-                BD_CUDA(cudaMemcpyAsync(d.phase.plume, d.plume_alt, sizeof(float) * nv, cudaMemcpyDeviceToDevice, st));
-        }
+                BD_CUDA(cudaMemcpyAsync(d.phase.plume, d.plume_alt, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
+            return BD_OK;
+        });
+        if (rc) return rc;
     }
     mark(e, st, 2);
-    int rc = phase_launch(e->pa, 1, st);
+    rc = run_stage(e, e->g_end, nullptr, 0, graphs, st, [&](cudaStream_t s) -> int {
+        return phase_launch(e->pa, BD_PHASE_FULL, s);
+    });
     if (e->timed) cudaEventRecord(e->ev[3], st);
     if (e->ring_on && e->timed) {
         cudaEvent_t ev = ring_event(e);
@@ -278,7 +352,7 @@ extern "C" int bd_engine_epoch_end(BdEngine* e, void* stream) {
     cudaStream_t st = as_stream(stream);
     k_epoch_end_only<<<1, 32, 0, st>>>(e->dyn);
     BD_CHECK_LAUNCH("k_epoch_end_only");
-    return phase_launch(e->pa, 1, st);
+    return phase_launch(e->pa, BD_PHASE_FULL, st);
 }
 
 extern "C" int bd_engine_read_diag(BdEngine* e, BdEpochDiag* out, void* stream) {

@@ -24,6 +24,8 @@ struct EngineDyn {
     float t_now;          // t as float for the kernels
     float _pad;
     long long mc_offset;  // photon-stream offset of this epoch's MC
+    int void_zlimit;      // 1 + deepest slice holding a void voxel (monotone: ablation is irreversible)
+    int _pad2;
 };
 
 struct PhaseArgs {
@@ -45,14 +47,16 @@ struct PhaseArgs {
     EngineDyn* dyn;
 };
 
-int phase_launch(const PhaseArgs& a, int with_plume_pass, cudaStream_t st);
+#define BD_PHASE_FULL 0  // phase update + removal + breach + void/plume/props pass
+#define BD_PHASE_INIT 1  // breach check (gap_open) + void/plume/props pass only
+int phase_launch(const PhaseArgs& a, int mode, cudaStream_t st);
 int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, float* H, float* Om, float* Chi,
                     const uint8_t* F, const float* src, const float* K, const float* R, cudaStream_t st);
 int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
-                 cudaStream_t st);
+                 cudaStream_t st, const int* zlimit, int full_first);
 int plume_policy_steps(const BdPlumeParams* p, int* n_steps, float* dt_step, float* decay_step);
 int mc_launch(const BdMcParams* p, const float* props, const uint8_t* flags, float* A, float* L, double* latz,
               double* ledger, unsigned long long* queue, double* partials, int max_blocks, int sm_count,
-              cudaStream_t st);
+              cudaStream_t st, const long long* offset_dev);
 
 }  // namespace bd

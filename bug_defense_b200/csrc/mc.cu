@@ -22,6 +22,8 @@
 
 #include <stdlib.h>
 
+#include <algorithm>
+
 namespace bd {
 
 struct McDev {
@@ -140,9 +142,12 @@ __device__ __forceinline__ void beam_offsets(const McDev& P, PhotonRng& rng, flo
     u1 = r * c; u2 = r * s;
 }
 
+// Per-thread FP64 accumulator for the per-collision channel (absorbed weight); the rare
+// channels (exits, roulette, truncation, absorption in void) go straight to the block's
+// partial row with FP64 atomics, so no block-wide barrier is needed anywhere in the kernel.
 struct ThreadLedger {
-    double absorbed, absorbed_void, gain;
-    unsigned long long collisions, crossings, reflections;
+    double absorbed;
+    unsigned collisions, crossings, reflections;
 };
 
 template <int DEPTH>  // 2: launch along +z at z=0 ; 0: launch along +x at x=0
@@ -197,8 +202,8 @@ __device__ __forceinline__ void trace_photon(const McDev& P, long long pid, cons
     }
     float ux = P.ux0, uy = P.uy0, uz = P.uz0;
     const int ny = P.ny, nz = P.nz;
-    const size_t sx_stride = (size_t)ny * nz;
-    size_t idx = (size_t)ix * sx_stride + (size_t)iy * nz + iz;
+    const int sx_stride = ny * nz;
+    int idx = ix * sx_stride + iy * nz + iz;
 
     // entrance face: deterministic specular split + refraction (voxel_mc_3d.py:183-192)
     float4 pr = __ldg(&props[idx]);
@@ -207,8 +212,9 @@ __device__ __forceinline__ void trace_photon(const McDev& P, long long pid, cons
         float n_in = pr.w;
         float cos_in = (DEPTH == 2) ? uz : ux;
         float r = fresnel_unpol(P.n_amb, n_in, cos_in, P.eq_eps);
-        atomicAdd(&sl[BD_LEDGER_SPECULAR], (double)r);
         w = 1.0f - r;
+        // the ledger books what the FP32 weight actually lost, so it closes exactly
+        atomicAdd(&sl[BD_LEDGER_SPECULAR], 1.0 - (double)w);
         if (w <= 0.0f) return;
         if (fabsf(n_in - P.n_amb) > P.entry_eps) refract_axis(ux, uy, uz, DEPTH, P.n_amb / n_in);
     }
@@ -218,9 +224,8 @@ __device__ __forceinline__ void trace_photon(const McDev& P, long long pid, cons
     float tau = -__logf(fmaxf(rng.uniform(), 1e-12f));
 
     const float dx = P.dx, dy = P.dy, dz = P.dz;
-    unsigned long long ncol = 0, ncross = 0, nrefl = 0;
-    long long ev = 0;
-    for (; ev < P.max_events; ++ev) {
+    unsigned ncol = 0, ncross = 0, nrefl = 0;
+    for (int ev = 0; ev < P.max_events; ++ev) {
         // exact ray/box distance to the exit face (voxel_mc_3d.py:72-98)
         float sx = ux > 1e-15f ? ((float)(ix + 1) * dx - x) * iux : (ux < -1e-15f ? ((float)ix * dx - x) * iux : 1e30f);
         float sy = uy > 1e-15f ? ((float)(iy + 1) * dy - y) * iuy : (uy < -1e-15f ? ((float)iy * dy - y) * iuy : 1e30f);
@@ -248,16 +253,19 @@ __device__ __forceinline__ void trace_photon(const McDev& P, long long pid, cons
                 }
             }
             {
-                float dw = w * pr.y;
-                w -= dw;
+                const float dw = w * pr.y;
+                const float w_new = w - dw;
                 atomicAdd(&A[idx], dw);
-                if (flags != nullptr && (__ldg(&flags[idx]) & BD_FLAG_ABLATED)) tl.absorbed_void += (double)dw;
-                else tl.absorbed += (double)dw;
+                const double lost = (double)w - (double)w_new;  // exact: both are FP32 values
+                if (flags != nullptr && (__ldg(&flags[idx]) & BD_FLAG_ABLATED)) atomicAdd(&sl[BD_LEDGER_ABSORBED_VOID], lost);
+                else tl.absorbed += lost;
+                w = w_new;
             }
             if (w < 1e-4f) {
                 if (rng.uniform() < 0.1f) {
-                    tl.gain += 9.0 * (double)w;
-                    w *= 10.0f;
+                    const float w10 = w * 10.0f;
+                    atomicAdd(&sl[BD_LEDGER_ROULETTE_GAIN], (double)w10 - (double)w);
+                    w = w10;
                 } else {
                     atomicAdd(&sl[BD_LEDGER_ROULETTE_LOSS], (double)w);
                     goto done;
@@ -315,7 +323,7 @@ __device__ __forceinline__ void trace_photon(const McDev& P, long long pid, cons
             }
         }
         {
-            size_t jidx = (size_t)jx * sx_stride + (size_t)jy * nz + jz;
+            const int jidx = jx * sx_stride + jy * nz + jz;
             float4 pn = __ldg(&props[jidx]);
             float n1 = pr.w, n2 = pn.w;
             if (fabsf(n1 - n2) > P.step_eps) {
@@ -347,17 +355,18 @@ done:
 }
 
 template <int DEPTH>
-__global__ void __launch_bounds__(128) k_mc_trace(McDev P, const float4* __restrict__ props,
-                                                  const uint8_t* __restrict__ flags, float* __restrict__ A,
-                                                  float* __restrict__ L, double* __restrict__ latz,
-                                                  unsigned long long* __restrict__ queue,
-                                                  double* __restrict__ partials) {
-    __shared__ double sl[BD_LEDGER_LEN];
-    if (threadIdx.x < BD_LEDGER_LEN) sl[threadIdx.x] = 0.0;
-    __syncthreads();
+__global__ void __launch_bounds__(128, 8) k_mc_trace(McDev P, const float4* __restrict__ props,
+                                                     const uint8_t* __restrict__ flags, float* __restrict__ A,
+                                                     float* __restrict__ L, double* __restrict__ latz,
+                                                     unsigned long long* __restrict__ queue,
+                                                     double* __restrict__ partials,
+                                                     const long long* __restrict__ offset_dev) {
+    // a photon-stream offset kept in device memory lets a captured graph advance it per replay
+    if (offset_dev != nullptr) P.offset += *offset_dev;
+    double* sl = partials + (size_t)blockIdx.x * BD_LEDGER_LEN;  // zeroed before the launch
     ThreadLedger tl;
-    tl.absorbed = tl.absorbed_void = tl.gain = 0.0;
-    tl.collisions = tl.crossings = tl.reflections = 0ull;
+    tl.absorbed = 0.0;
+    tl.collisions = tl.crossings = tl.reflections = 0u;
 
     const unsigned long long N = (unsigned long long)P.n_photons;
     for (;;) {
@@ -365,28 +374,24 @@ __global__ void __launch_bounds__(128) k_mc_trace(McDev P, const float4* __restr
         if (p >= N) break;
         trace_photon<DEPTH>(P, (long long)p, props, flags, A, L, latz, sl, tl);
     }
-    // warp reduction of the per-thread channels
-    double v0 = tl.absorbed, v1 = tl.absorbed_void, v2 = tl.gain;
-    unsigned long long c0 = tl.collisions, c1 = tl.crossings, c2 = tl.reflections;
+    // warp reduction of the per-thread channels, one FP64 atomic per warp and channel
+    double v0 = tl.absorbed;
+    unsigned c0 = tl.collisions, c1 = tl.crossings, c2 = tl.reflections;
+    __syncwarp();  // every lane reaches here (no early return): reconverge for the shuffles
+    const unsigned mask = 0xffffffffu;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        v0 += __shfl_xor_sync(0xffffffffu, v0, o);
-        v1 += __shfl_xor_sync(0xffffffffu, v1, o);
-        v2 += __shfl_xor_sync(0xffffffffu, v2, o);
-        c0 += __shfl_xor_sync(0xffffffffu, c0, o);
-        c1 += __shfl_xor_sync(0xffffffffu, c1, o);
-        c2 += __shfl_xor_sync(0xffffffffu, c2, o);
+        v0 += __shfl_xor_sync(mask, v0, o);
+        c0 += __shfl_xor_sync(mask, c0, o);
+        c1 += __shfl_xor_sync(mask, c1, o);
+        c2 += __shfl_xor_sync(mask, c2, o);
     }
     if ((threadIdx.x & 31) == 0) {
         atomicAdd(&sl[BD_LEDGER_ABSORBED], v0);
-        atomicAdd(&sl[BD_LEDGER_ABSORBED_VOID], v1);
-        atomicAdd(&sl[BD_LEDGER_ROULETTE_GAIN], v2);
         atomicAdd(&sl[BD_LEDGER_COLLISIONS], (double)c0);
         atomicAdd(&sl[BD_LEDGER_CROSSINGS], (double)c1);
         atomicAdd(&sl[BD_LEDGER_REFLECTIONS], (double)c2);
     }
-    __syncthreads();
-    if (threadIdx.x < BD_LEDGER_LEN) partials[(size_t)blockIdx.x * BD_LEDGER_LEN + threadIdx.x] = sl[threadIdx.x];
 }
 
 // Fixed-order reduction of the per-block partials (deterministic for a given grid).
@@ -503,16 +508,26 @@ McDev mc_dev_params(const BdMcParams* p) {
 // Launch with caller-provided scratch (queue counter + per-block partials).
 int mc_launch(const BdMcParams* p, const float* props, const uint8_t* flags, float* A, float* L,
               double* latz, double* ledger, unsigned long long* queue, double* partials, int max_blocks,
-              int sm_count, cudaStream_t st) {
+              int sm_count, cudaStream_t st, const long long* offset_dev) {
     McDev d = mc_dev_params(p);
-    int blocks = (int)std::min<long long>((p->n_photons + 127) / 128, (long long)sm_count * 16);
+    static int per_sm[2] = {0, 0};
+    const int ax = p->launch_axis == 0 ? 0 : 1;
+    if (per_sm[ax] == 0) {
+        int nb = 0;
+        if (ax == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_mc_trace<2>, 128, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_mc_trace<0>, 128, 0);
+        per_sm[ax] = std::max(1, std::min(nb, 16));
+        cudaGetLastError();
+    }
+    int blocks = (int)std::min<long long>((p->n_photons + 127) / 128, (long long)sm_count * per_sm[ax]);
     blocks = std::max(1, std::min(blocks, max_blocks));
     BD_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st));
+    BD_CUDA(cudaMemsetAsync(partials, 0, sizeof(double) * BD_LEDGER_LEN * blocks, st));
     const float4* pr = reinterpret_cast<const float4*>(props);
     if (p->launch_axis == 0)
-        k_mc_trace<2><<<blocks, 128, 0, st>>>(d, pr, flags, A, L, latz, queue, partials);
+        k_mc_trace<2><<<blocks, 128, 0, st>>>(d, pr, flags, A, L, latz, queue, partials, offset_dev);
     else
-        k_mc_trace<0><<<blocks, 128, 0, st>>>(d, pr, flags, A, L, latz, queue, partials);
+        k_mc_trace<0><<<blocks, 128, 0, st>>>(d, pr, flags, A, L, latz, queue, partials, offset_dev);
     BD_CHECK_LAUNCH("k_mc_trace");
     k_ledger_reduce<<<1, 32, 0, st>>>(partials, blocks, (double)p->n_photons, ledger);
     BD_CHECK_LAUNCH("k_ledger_reduce");
@@ -528,7 +543,7 @@ extern "C" int bd_mc_trace(BdMcContext* c, const BdMcParams* p, const float* pro
     BD_REQUIRE(props != nullptr && A != nullptr && ledger != nullptr, "bd_mc_trace: props, A and ledger are required");
     BD_REQUIRE(!(p->options & BD_MC_TALLY_FLUENCE) || L != nullptr, "bd_mc_trace: BD_MC_TALLY_FLUENCE needs L");
     return mc_launch(p, props, flags, A, L, lat_depth, ledger, c->queue, c->partials, c->partial_blocks,
-                     c->sm_count, as_stream(stream));
+                     c->sm_count, as_stream(stream), nullptr);
 }
 
 extern "C" int bd_mc_pack_props(const float* mu_a, const float* mu_s, const float* g, const float* n,

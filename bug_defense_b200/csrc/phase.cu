@@ -144,6 +144,7 @@ __global__ void __launch_bounds__(256) k_void_plume(PhaseArgs a, long long nv) {
     const int mid_col = (a.nx / 2) * a.ny + a.ny / 2;
     double tau_sum = 0.0, abl_sum = 0.0, abl_cnt = 0.0;
     float peak = 0.0f;
+    int kmax = -1;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv;
          i += (long long)gridDim.x * blockDim.x) {
         uint8_t f = a.flags[i];
@@ -152,6 +153,7 @@ __global__ void __launch_bounds__(256) k_void_plume(PhaseArgs a, long long nv) {
         const bool vd = ablated || (gap_open && k >= a.gap_k0 && k < a.gap_k1);
         f = vd ? (uint8_t)(f | BD_FLAG_VOID) : (uint8_t)(f & ~BD_FLAG_VOID);
         a.flags[i] = f;
+        if (vd) kmax = max(kmax, k);
         float mu_ext = 0.0f;
         if (a.has_plume) {
             float raw = a.plume[i];
@@ -183,6 +185,9 @@ __global__ void __launch_bounds__(256) k_void_plume(PhaseArgs a, long long nv) {
     double s2 = block_sum(abl_cnt, shd);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) peak = fmaxf(peak, __shfl_xor_sync(0xffffffffu, peak, o));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+    if ((threadIdx.x & 31) == 0 && kmax >= 0) atomicMax(&a.dyn->void_zlimit, kmax + 1);
     __shared__ float shp[8];
     if ((threadIdx.x & 31) == 0) shp[threadIdx.x >> 5] = peak;
     __syncthreads();
@@ -197,19 +202,19 @@ __global__ void __launch_bounds__(256) k_void_plume(PhaseArgs a, long long nv) {
     }
 }
 
-int phase_launch(const PhaseArgs& a, int with_plume_pass, cudaStream_t st) {
+int phase_launch(const PhaseArgs& a, int mode, cudaStream_t st) {
     const long long nv = (long long)a.nx * a.ny * a.nz;
     const int blocks = grid_for(nv, 256, 148 * 16);
-    k_phase_remove<<<blocks, 256, 0, st>>>(a, nv);
-    BD_CHECK_LAUNCH("k_phase_remove");
+    if (mode == BD_PHASE_FULL) {
+        k_phase_remove<<<blocks, 256, 0, st>>>(a, nv);
+        BD_CHECK_LAUNCH("k_phase_remove");
+    }
     if (a.gap_k0 > 0) {
         k_gap_breach<<<grid_for((long long)a.nx * a.ny, 128, 148 * 8), 128, 0, st>>>(a);
         BD_CHECK_LAUNCH("k_gap_breach");
     }
-    if (with_plume_pass) {
-        k_void_plume<<<blocks, 256, 0, st>>>(a, nv);
-        BD_CHECK_LAUNCH("k_void_plume");
-    }
+    k_void_plume<<<blocks, 256, 0, st>>>(a, nv);
+    BD_CHECK_LAUNCH("k_void_plume");
     return BD_OK;
 }
 

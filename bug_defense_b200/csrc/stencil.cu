@@ -28,7 +28,10 @@ struct Geo {
     float idx2, idy2, idz2, dz, h_eff, t_amb, dt;
 };
 
-__device__ __forceinline__ float kface(float a, float b) { return 2.0f * a * b / (a + b + 1e-12f); }
+// Harmonic face conductance 2 k_c k_n / (k_c + k_n + 1e-12). The quotient uses the fast
+// reciprocal path (<= 2 ulp): six precise IEEE divisions per voxel made the stencil
+// instruction-bound, while the parity bar on T is 1e-4 relative.
+__device__ __forceinline__ float kface(float a, float b) { return __fdividef(2.0f * a * b, a + b + 1e-12f); }
 
 template <int BC>
 __device__ __forceinline__ float zwall_flux(float Tc, float kc, const Geo& g) {
@@ -50,6 +53,8 @@ struct AblConst {
 };
 
 // MODE 0: thermal only. MODE 1: fused ablation substep.
+// Each thread marches NI x-planes of one (y, z) column; T and k of plane i+2 are prefetched
+// while plane i is computed so two DRAM round trips are in flight per thread.
 template <int MODE, int BC, bool ARR, bool CHAR>
 __global__ void __launch_bounds__(TZ * TY) k_substep(Geo g, AblConst c, const float* __restrict__ T,
                                                      float* __restrict__ Tn, const float* __restrict__ src,
@@ -61,19 +66,26 @@ __global__ void __launch_bounds__(TZ * TY) k_substep(Geo g, AblConst c, const fl
     if (k >= g.nz || j >= g.ny) return;
     const int i0 = blockIdx.z * g.ni;
     const int i1 = min(i0 + g.ni, g.nx);
-    const size_t plane = (size_t)g.ny * g.nz;
-    const size_t base = (size_t)j * g.nz + k;
+    const int plane = g.ny * g.nz;
+    const int base = j * g.nz + k;
 
-    float Tm = 0.0f, km = 0.0f;
-    size_t idx = (size_t)i0 * plane + base;
+    int idx = i0 * plane + base;
+    float Tm = 0.0f, km = 0.0f, Tp = 0.0f, kp = 0.0f;
     float Tc = __ldg(&T[idx]), kc = __ldg(&K[idx]);
     if (i0 > 0) { Tm = __ldg(&T[idx - plane]); km = __ldg(&K[idx - plane]); }
+    if (i0 + 1 < g.nx) { Tp = __ldg(&T[idx + plane]); kp = __ldg(&K[idx + plane]); }
 
     for (int i = i0; i < i1; ++i, idx += plane) {
-        float Tp = 0.0f, kp = 0.0f;
-        const bool has_e = (i + 1 < g.nx);
-        if (has_e) { Tp = __ldg(&T[idx + plane]); kp = __ldg(&K[idx + plane]); }
+        // prefetch plane i+2 (the x+1 neighbour of the next iteration)
+        float Tq = 0.0f, kq = 0.0f;
+        if (i + 2 < g.nx && i + 1 < i1) { Tq = __ldg(&T[idx + 2 * plane]); kq = __ldg(&K[idx + 2 * plane]); }
+        const float rho = __ldg(&R[idx]);
+        uint8_t f = 0;
+        if (MODE == 1) f = __ldg(&F[idx]);
+        float q = 0.0f;
+        if (c.is_active) q = __ldg(&src[idx]);
 
+        const bool has_e = (i + 1 < g.nx);
         float fw = (i > 0) ? kface(kc, km) * (Tm - Tc) * g.idx2 : 0.0f;
         float fe = has_e ? kface(kc, kp) * (Tp - Tc) * g.idx2 : 0.0f;
         float fs = 0.0f, fn = 0.0f, ft, fb;
@@ -85,16 +97,10 @@ __global__ void __launch_bounds__(TZ * TY) k_substep(Geo g, AblConst c, const fl
         else              fb = zwall_flux<BC>(Tc, kc, g);
         const float div = fw + fe + fs + fn + ft + fb;
 
-        const float rho = __ldg(&R[idx]);
         const float cap = fmaxf(rho, 1e-12f);
-        uint8_t f = 0;
-        if (MODE == 1) f = __ldg(&F[idx]);
-        float q = 0.0f;
-        if (c.is_active) {
-            q = __ldg(&src[idx]) * c.q_scale;
-            if (MODE == 1 && c.zero_src_in_ablated && (f & BD_FLAG_ABLATED)) q = 0.0f;
-        }
-        float Tt = Tc + g.dt * (div + q) / cap;
+        q *= c.q_scale;
+        if (MODE == 1 && c.zero_src_in_ablated && (f & BD_FLAG_ABLATED)) q = 0.0f;
+        float Tt = Tc + __fdividef(g.dt * (div + q), cap);
 
         if (MODE == 1) {
             const bool abl = (f & BD_FLAG_ABLATED) != 0;
@@ -121,7 +127,7 @@ __global__ void __launch_bounds__(TZ * TY) k_substep(Geo g, AblConst c, const fl
             }
         }
         Tn[idx] = Tt;
-        Tm = Tc; km = kc; Tc = Tp; kc = kp;
+        Tm = Tc; km = kc; Tc = Tp; kc = kp; Tp = Tq; kp = kq;
     }
 }
 
@@ -130,21 +136,29 @@ struct PlumeConst {
     float vz_over_dz, dtp, decay;
 };
 
-// One FTCS plume step over the whole grid (plume.py:46-80).
-__global__ void __launch_bounds__(TZ * TY) k_plume_step(int nx, int ny, int nz, int ni, PlumeConst c,
+// One FTCS plume step (plume.py:46-80). CTA (y tile, x plane); the z loop runs over 32-slice
+// tiles of k < zlim, zlim = *zlimit when given (every void voxel lies above it) else nz.
+// Non-void voxels are written (as 0) only when full_write is set: the engine keeps them 0 in
+// both ping-pong buffers, so a step touches only the void domain plus one flag byte per voxel.
+__global__ void __launch_bounds__(TZ * TY) k_plume_step(int nx, int ny, int nz, PlumeConst c,
                                                         const float* __restrict__ C, float* __restrict__ Cn,
-                                                        const uint8_t* __restrict__ F) {
-    const int k = blockIdx.x * TZ + threadIdx.x;
-    const int j = blockIdx.y * TY + threadIdx.y;
-    if (k >= nz || j >= ny) return;
-    const int i0 = blockIdx.z * ni;
-    const int i1 = min(i0 + ni, nx);
-    const size_t plane = (size_t)ny * nz;
-    size_t idx = (size_t)i0 * plane + (size_t)j * nz + k;
-    const bool jk_wall = (j == 0 || j == ny - 1 || k == 0 || k == nz - 1);
-    for (int i = i0; i < i1; ++i, idx += plane) {
+                                                        const uint8_t* __restrict__ F,
+                                                        const int* __restrict__ zlimit, int full_write) {
+    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
+    const int j = blockIdx.x * TY + threadIdx.y;
+    const int i = blockIdx.y;
+    if (j >= ny) return;
+    const int plane = ny * nz;
+    const bool xy_wall = (i == 0 || i == nx - 1 || j == 0 || j == ny - 1);
+    const int col = i * plane + j * nz;
+    for (int k = threadIdx.x; k < zl; k += TZ) {
+        const int idx = col + k;
         const uint8_t f = __ldg(&F[idx]);
-        if (!(f & BD_FLAG_VOID) || jk_wall || i == 0 || i == nx - 1) {
+        if (!(f & BD_FLAG_VOID)) {
+            if (full_write) Cn[idx] = 0.0f;
+            continue;
+        }
+        if (xy_wall || k == 0 || k == nz - 1) {
             Cn[idx] = 0.0f;
             continue;
         }
@@ -178,11 +192,13 @@ static dim3 tile_grid(int nx, int ny, int nz, int ni) {
 }
 
 static int pick_ni(int nx, int ny, int nz) {
-    // aim for ~8 resident CTAs of 256 threads on each of 148 SMs
+    // short marches (~8 planes) and several waves of 256-thread CTAs: enough independent
+    // DRAM round trips in flight to cover latency without a long serial chain per thread
     long long cols = (long long)((nz + TZ - 1) / TZ) * ((ny + TY - 1) / TY);
-    long long want = 148LL * 8;
+    long long want = 148LL * 6 * 4;
     long long chunks = std::max(1LL, want / std::max(1LL, cols));
     int ni = (int)std::max(4LL, ((long long)nx + chunks - 1) / chunks);
+    ni = std::min(ni, 8);
     return std::min(ni, std::max(nx, 1));
 }
 
@@ -251,6 +267,7 @@ extern "C" int bd_thermal_advance(const BdThermalParams* p, float* Ta, float* Tb
     BD_REQUIRE(!p->is_active || src != nullptr, "bd_thermal_advance: active source needs src");
     BD_REQUIRE(p->bc_mode == BD_BC_SERIES || p->bc_mode == BD_BC_METAL, "bd_thermal_advance: bad bc_mode");
     BD_REQUIRE(n >= 0, "bd_thermal_advance: n_substeps must be >= 0");
+    BD_REQUIRE((long long)p->nx * p->ny * p->nz < (1LL << 31), "bd_thermal_advance: grid exceeds 2^31 voxels");
     if (n == 0) return BD_OK;
     Geo g = make_geo(p->nx, p->ny, p->nz, p->dx, p->dy, p->dz, p->dt, p->h_eff, p->t_ambient);
     AblConst c{};
@@ -293,7 +310,7 @@ int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, floa
 }
 
 int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
-                 cudaStream_t st) {
+                 cudaStream_t st, const int* zlimit, int full_first) {
     int steps;
     float dtp, decay;
     int rc = plume_policy_steps(p, &steps, &dtp, &decay);
@@ -305,13 +322,13 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     c.vz_over_dz = p->vz > 0.0f ? p->vz / p->dz : 0.0f;
     c.dtp = dtp;
     c.decay = decay;
-    const int ni = pick_ni(p->nx, p->ny, p->nz);
-    dim3 grid = tile_grid(p->nx, p->ny, p->nz, ni), block(TZ, TY);
+    const dim3 grid((p->ny + TY - 1) / TY, p->nx);
     const long long total = (long long)steps * n_substeps;
     for (long long s = 0; s < total; ++s) {
         const float* in = (s & 1) ? Cb : Ca;
         float* out = (s & 1) ? Ca : Cb;
-        k_plume_step<<<grid, block, 0, st>>>(p->nx, p->ny, p->nz, ni, c, in, out, F);
+        const int full = (full_first && s < 2) ? 1 : 0;
+        k_plume_step<<<grid, dim3(TZ, TY), 0, st>>>(p->nx, p->ny, p->nz, c, in, out, F, zlimit, full);
     }
     BD_CHECK_LAUNCH("k_plume_step");
     if (in_b) *in_b = (int)(total & 1);
@@ -329,6 +346,7 @@ extern "C" int bd_ablation_advance(const BdAblationParams* p, float* Ta, float* 
     BD_REQUIRE(!p->has_arrhenius || Om != nullptr, "bd_ablation_advance: Arrhenius needs Omega");
     BD_REQUIRE(!p->has_char || Chi != nullptr, "bd_ablation_advance: char kinetics need chi");
     BD_REQUIRE(n >= 0, "bd_ablation_advance: n_substeps must be >= 0");
+    BD_REQUIRE((long long)p->nx * p->ny * p->nz < (1LL << 31), "bd_ablation_advance: grid exceeds 2^31 voxels");
     if (n == 0) return BD_OK;
     return ablation_launch(p, Ta, Tb, n, H, Om, Chi, F, src, K, R, as_stream(stream));
 }
@@ -339,11 +357,14 @@ extern "C" int bd_plume_advance(const BdPlumeParams* p, float* Ca, float* Cb, in
     BD_REQUIRE(p->nx > 0 && p->ny > 0 && p->nz > 0, "bd_plume_advance: grid dims must be positive");
     BD_REQUIRE(Ca && Cb && F, "bd_plume_advance: NULL field");
     BD_REQUIRE(n_substeps >= 0, "bd_plume_advance: n_substeps must be >= 0");
+    BD_REQUIRE((long long)p->nx * p->ny * p->nz < (1LL << 31), "bd_plume_advance: grid exceeds 2^31 voxels");
     if (n_substeps == 0) {
         if (in_b) *in_b = 0;
         return BD_OK;
     }
-    return plume_launch(p, Ca, Cb, n_substeps, F, in_b, as_stream(stream));
+    // the context API may hold arbitrary values in non-void voxels: the first two steps write
+    // every voxel (one per ping-pong buffer), later steps touch the void domain only
+    return plume_launch(p, Ca, Cb, n_substeps, F, in_b, as_stream(stream), nullptr, 1);
 }
 
 extern "C" int bd_plume_steps_per_substep(const BdPlumeParams* p, int* n_steps, float* dt_step) {

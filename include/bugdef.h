@@ -270,6 +270,7 @@ typedef struct BdEpochDiag {
 } BdEpochDiag;
 
 #define BD_EPOCH_SKIP_MC 0x1       /* use the absorbed map already in A (no MC this epoch) */
+#define BD_EPOCH_NO_GRAPH 0x2      /* launch the stages directly instead of as CUDA graphs  */
 
 typedef struct BdEngine BdEngine;
 /* Replaces CoupledAblationEngine.__init__ device setup (coupled_ablation.py:184-407);

@@ -26,9 +26,10 @@ def _engine(gpu, g, **extra):
     return eng, cfg
 
 
-def test_engine_matches_reference_with_fixed_source(gpu, golden):
+@pytest.mark.parametrize("use_graphs", [True, False])
+def test_engine_matches_reference_with_fixed_source(gpu, golden, use_graphs):
     g = golden("engine_fixedQ.npz")
-    eng, cfg = _engine(gpu, g)
+    eng, cfg = _engine(gpu, g, use_graphs=use_graphs)
     A = g["in_A"]
     diag = []
     snaps = {int(e) for e in g["snap_epochs"]}

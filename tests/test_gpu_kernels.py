@@ -181,5 +181,7 @@ def test_phase_update_matches_reference(gpu, golden, name):
     for k_in, k_out in (("H", "out_H"), ("mu_a", "out_mu_a"), ("mu_s", "out_mu_s"), ("g", "out_g"), ("n", "out_n"),
                         ("k", "out_k"), ("rho", "out_rho")):
         got = fields[k_in].double().cpu().numpy()
-        ok = np.isclose(got, g[k_out], rtol=2e-6, atol=1e-12) | near
+        # FP32 interpolation: error relative to the magnitudes interpolated between
+        scale = max(np.max(np.abs(g[k_out])), np.max(np.abs(ins[k_in])))
+        ok = np.isclose(got, g[k_out], rtol=2e-6, atol=4e-7 * scale) | near
         assert np.all(ok), (k_in, np.max(np.abs(got - g[k_out])))

@@ -16,7 +16,8 @@ def test_gpu_mc_matches_reference_statistics(gpu, orc, golden, name):
     r = gpu.run_voxel_mc3d(n_photons=n, base_seed=4321, **kw)
     assert r["engine"] == "gpu"
     for key, (mean, se) in stats["stats"].items():
-        tol = 3.5 * np.sqrt(2.0) * se + 1e-9
+        # deterministic channels (R_spec) differ by FP32 rounding only
+        tol = 3.5 * np.sqrt(2.0) * se + 1e-6
         assert abs(r["spectro_raw"][key] - mean) <= tol, (key, r["spectro_raw"][key], mean, tol)
     # FP64 ledger closes to round-off once roulette and truncation are accounted
     assert abs(r["ledger_closure"] - 1.0) < 1e-9
