@@ -193,6 +193,8 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     global _lib
     if _lib is not None and path is None:
         return _lib
+    if path is None and os.environ.get("BUGDEF_LIB"):
+        path = os.environ["BUGDEF_LIB"]  # another build of the same library (tuning variants)
     p = Path(path) if path is not None else LIB_PATH
     if not p.exists():
         raise RuntimeError(f"libbugdef.so not built ({p}); run `python -m bug_defense_b200.build`")
@@ -201,7 +203,7 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if path is None:
+    if _lib is None:
         _lib = lib
     return lib
 

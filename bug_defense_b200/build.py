@@ -39,17 +39,18 @@ def _digest(extra_flags) -> str:
     return h.hexdigest()[:16]
 
 
-def build(force: bool = False, verbose: bool = False, extra_flags=()) -> Path:
+def build(force: bool = False, verbose: bool = False, extra_flags=(), out: Path | None = None) -> Path:
     """Compile every .cu source for sm_100a and link libbugdef.so (skipped when up to date)."""
-    OUT_DIR.mkdir(exist_ok=True)
-    stamp = OUT_DIR / "libbugdef.stamp"
+    lib = Path(out) if out is not None else LIB
+    lib.parent.mkdir(parents=True, exist_ok=True)
+    stamp = lib.with_suffix(".stamp")
     dig = _digest(list(extra_flags))
-    if not force and LIB.exists() and stamp.exists() and stamp.read_text() == dig:
-        return LIB
+    if not force and lib.exists() and stamp.exists() and stamp.read_text() == dig:
+        return lib
     srcs = [str(CSRC / s) for s in SOURCES if (CSRC / s).exists()]
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
            "-Xcompiler", "-fvisibility=hidden", "-I", str(ROOT / "include"), "-I", str(CSRC),
-           "--expt-relaxed-constexpr", "-lcuda", *extra_flags, "-o", str(LIB) + ".tmp", *srcs]
+           "--expt-relaxed-constexpr", "-lcuda", *extra_flags, "-o", str(lib) + ".tmp", *srcs]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     res = subprocess.run(cmd, capture_output=True, text=True)
@@ -57,9 +58,9 @@ def build(force: bool = False, verbose: bool = False, extra_flags=()) -> Path:
         raise RuntimeError(f"nvcc failed ({res.returncode}):\n{res.stderr}")
     if verbose and res.stderr:
         print(res.stderr, file=sys.stderr)
-    os.replace(str(LIB) + ".tmp", LIB)
+    os.replace(str(lib) + ".tmp", lib)
     stamp.write_text(dig)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

@@ -22,6 +22,7 @@ struct BdEngine {
     BdEngineDesc d;
     cudaStream_t cap_stream = nullptr;  // private stream used only to capture stage graphs
     StageGraph g_mc, g_sub_on, g_sub_off, g_plume, g_end;
+    uint8_t* plume_mask = nullptr;      // plume neighbourhood bytes (rebuilt every epoch)
     bd::PhaseArgs pa;
     bd::EngineDyn* dyn = nullptr;      // device
     bd::EngineDyn* dyn_host = nullptr; // pinned
@@ -196,6 +197,8 @@ extern "C" int bd_engine_create(const BdEngineDesc* desc, BdEngine** out) {
     if (err == cudaSuccess) err = cudaMemset(e->dyn, 0, sizeof(EngineDyn));
     for (int q = 0; q < 4 && err == cudaSuccess; ++q) err = cudaEventCreate(&e->ev[q]);
     if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->cap_stream, cudaStreamNonBlocking);
+    if (err == cudaSuccess && desc->has_plume_transport)
+        err = cudaMalloc(&e->plume_mask, (size_t)desc->phase.nx * desc->phase.ny * desc->phase.nz);
     if (err != cudaSuccess) {
         bd_engine_destroy(e);
         return cuda_status(err, "bd_engine_create");
@@ -228,6 +231,7 @@ extern "C" int bd_engine_destroy(BdEngine* e) {
     graph_reset(e->g_mc); graph_reset(e->g_sub_on); graph_reset(e->g_sub_off);
     graph_reset(e->g_plume); graph_reset(e->g_end);
     if (e->cap_stream) cudaStreamDestroy(e->cap_stream);
+    cudaFree(e->plume_mask);
     delete e;
     return BD_OK;
 }
@@ -294,7 +298,7 @@ extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void*
         rc = run_stage(e, e->g_plume, &d.plume, sizeof(d.plume), graphs, st, [&](cudaStream_t s) -> int {
             int in_b = 0;
             int r = plume_launch(&d.plume, d.phase.plume, d.plume_alt, d.n_substeps, d.phase.flags, &in_b, s,
-                                 &e->dyn->void_zlimit, 0);
+                                 &e->dyn->void_zlimit, 0, e->plume_mask);
             if (r) return r;
             if (in_b)
                 BD_CUDA(cudaMemcpyAsync(d.phase.plume, d.plume_alt, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));

@@ -53,7 +53,7 @@ int phase_launch(const PhaseArgs& a, int mode, cudaStream_t st);
 int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, float* H, float* Om, float* Chi,
                     const uint8_t* F, const float* src, const float* K, const float* R, cudaStream_t st);
 int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
-                 cudaStream_t st, const int* zlimit, int full_first);
+                 cudaStream_t st, const int* zlimit, int full_first, uint8_t* mask);
 int plume_policy_steps(const BdPlumeParams* p, int* n_steps, float* dt_step, float* decay_step);
 int mc_launch(const BdMcParams* p, const float* props, const uint8_t* flags, float* A, float* L, double* latz,
               double* ledger, unsigned long long* queue, double* partials, int max_blocks, int sm_count,

@@ -354,8 +354,11 @@ done:
     tl.reflections += nrefl;
 }
 
+#ifndef BD_MC_MIN_BLOCKS
+#define BD_MC_MIN_BLOCKS 8
+#endif
 template <int DEPTH>
-__global__ void __launch_bounds__(128, 8) k_mc_trace(McDev P, const float4* __restrict__ props,
+__global__ void __launch_bounds__(128, BD_MC_MIN_BLOCKS) k_mc_trace(McDev P, const float4* __restrict__ props,
                                                      const uint8_t* __restrict__ flags, float* __restrict__ A,
                                                      float* __restrict__ L, double* __restrict__ latz,
                                                      unsigned long long* __restrict__ queue,

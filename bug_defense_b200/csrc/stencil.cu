@@ -136,43 +136,77 @@ struct PlumeConst {
     float vz_over_dz, dtp, decay;
 };
 
-// One FTCS plume step (plume.py:46-80). CTA (y tile, x plane); the z loop runs over 32-slice
-// tiles of k < zlim, zlim = *zlimit when given (every void voxel lies above it) else nz.
-// Non-void voxels are written (as 0) only when full_write is set: the engine keeps them 0 in
-// both ping-pong buffers, so a step touches only the void domain plus one flag byte per voxel.
+// Plume neighbourhood byte per voxel, rebuilt whenever the void domain changes (epoch end):
+//   bit 6: voxel is void            bit 7: voxel is void and not on an outer wall (FTCS update)
+//   bits 0-5: -x +x -y +y -z +z neighbour is void (otherwise its value is replaced by the centre,
+//   the zero-flux wall of plume.py:61-71)
+#define BD_PM_VOID 0x40u
+#define BD_PM_UPDATE 0x80u
+__global__ void k_plume_mask(int nx, int ny, int nz, const uint8_t* __restrict__ F, uint8_t* __restrict__ M,
+                             const int* __restrict__ zlimit) {
+    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
+    const int j = blockIdx.x * TY + threadIdx.y;
+    const int i = blockIdx.y;
+    if (j >= ny) return;
+    const int plane = ny * nz;
+    const bool xy_interior = (i > 0 && i < nx - 1 && j > 0 && j < ny - 1);
+    const int col = i * plane + j * nz;
+    for (int k = threadIdx.x; k < zl; k += TZ) {
+        const int idx = col + k;
+        uint8_t m = 0;
+        if (F[idx] & BD_FLAG_VOID) {
+            m = BD_PM_VOID;
+            if (xy_interior && k > 0 && k < nz - 1) {
+                m |= BD_PM_UPDATE;
+                m |= (F[idx - plane] & BD_FLAG_VOID) ? 0x01 : 0;
+                m |= (F[idx + plane] & BD_FLAG_VOID) ? 0x02 : 0;
+                m |= (F[idx - nz] & BD_FLAG_VOID) ? 0x04 : 0;
+                m |= (F[idx + nz] & BD_FLAG_VOID) ? 0x08 : 0;
+                m |= (F[idx - 1] & BD_FLAG_VOID) ? 0x10 : 0;
+                m |= (F[idx + 1] & BD_FLAG_VOID) ? 0x20 : 0;
+            }
+        }
+        M[idx] = m;
+    }
+}
+
+// One FTCS plume step (plume.py:46-80). CTA (y tile, x plane); a thread owns the voxels
+// k = tx, tx+32, ... < zlim of one (x, y) column, zlim = *zlimit when given (every void voxel
+// lies above it) else nz. The neighbourhood comes from the mask byte; the six neighbour values
+// are loaded unconditionally and selected, so no load depends on another. Non-void voxels are
+// written (as 0) only when full_write is set: the engine keeps them 0 in both ping-pong
+// buffers, so a step touches only the void domain plus one mask byte per voxel.
 __global__ void __launch_bounds__(TZ * TY) k_plume_step(int nx, int ny, int nz, PlumeConst c,
                                                         const float* __restrict__ C, float* __restrict__ Cn,
-                                                        const uint8_t* __restrict__ F,
+                                                        const uint8_t* __restrict__ M,
                                                         const int* __restrict__ zlimit, int full_write) {
     const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
     const int j = blockIdx.x * TY + threadIdx.y;
     const int i = blockIdx.y;
     if (j >= ny) return;
     const int plane = ny * nz;
-    const bool xy_wall = (i == 0 || i == nx - 1 || j == 0 || j == ny - 1);
     const int col = i * plane + j * nz;
     for (int k = threadIdx.x; k < zl; k += TZ) {
         const int idx = col + k;
-        const uint8_t f = __ldg(&F[idx]);
-        if (!(f & BD_FLAG_VOID)) {
-            if (full_write) Cn[idx] = 0.0f;
+        const uint8_t m = __ldg(&M[idx]);
+        if (!(m & BD_PM_UPDATE)) {
+            if ((m & BD_PM_VOID) || full_write) Cn[idx] = 0.0f;
             continue;
         }
-        if (xy_wall || k == 0 || k == nz - 1) {
-            Cn[idx] = 0.0f;
-            continue;
-        }
-        const float cc = __ldg(&C[idx]);
-        const float cw = (__ldg(&F[idx - plane]) & BD_FLAG_VOID) ? __ldg(&C[idx - plane]) : cc;
-        const float ce = (__ldg(&F[idx + plane]) & BD_FLAG_VOID) ? __ldg(&C[idx + plane]) : cc;
-        const float cs = (__ldg(&F[idx - nz]) & BD_FLAG_VOID) ? __ldg(&C[idx - nz]) : cc;
-        const float cn = (__ldg(&F[idx + nz]) & BD_FLAG_VOID) ? __ldg(&C[idx + nz]) : cc;
-        const float cb = (__ldg(&F[idx - 1]) & BD_FLAG_VOID) ? __ldg(&C[idx - 1]) : cc;
-        const float ct = (__ldg(&F[idx + 1]) & BD_FLAG_VOID) ? __ldg(&C[idx + 1]) : cc;
-        const float diff = c.dxy_x * (cw - 2.0f * cc + ce) + c.dxy_y * (cs - 2.0f * cc + cn) +
-                           c.dz_z * (cb - 2.0f * cc + ct);
-        const float adv = -c.vz_over_dz * (cc - ct);
-        const float v = (cc + c.dtp * (diff + adv)) * c.decay;
+        const float c0 = __ldg(&C[idx]);
+        const float cw = __ldg(&C[idx - plane]), ce = __ldg(&C[idx + plane]);
+        const float cs = __ldg(&C[idx - nz]), cn = __ldg(&C[idx + nz]);
+        const float cb = __ldg(&C[idx - 1]), ct = __ldg(&C[idx + 1]);
+        const float w = (m & 0x01) ? cw : c0;
+        const float e = (m & 0x02) ? ce : c0;
+        const float sx = (m & 0x04) ? cs : c0;
+        const float nn = (m & 0x08) ? cn : c0;
+        const float b = (m & 0x10) ? cb : c0;
+        const float t = (m & 0x20) ? ct : c0;
+        const float diff = c.dxy_x * (w - 2.0f * c0 + e) + c.dxy_y * (sx - 2.0f * c0 + nn) +
+                           c.dz_z * (b - 2.0f * c0 + t);
+        const float adv = -c.vz_over_dz * (c0 - t);
+        const float v = (c0 + c.dtp * (diff + adv)) * c.decay;
         Cn[idx] = fmaxf(v, 0.0f);
     }
 }
@@ -198,7 +232,10 @@ static int pick_ni(int nx, int ny, int nz) {
     long long want = 148LL * 6 * 4;
     long long chunks = std::max(1LL, want / std::max(1LL, cols));
     int ni = (int)std::max(4LL, ((long long)nx + chunks - 1) / chunks);
-    ni = std::min(ni, 8);
+#ifndef BD_STENCIL_NI
+#define BD_STENCIL_NI 8
+#endif
+    ni = std::min(ni, BD_STENCIL_NI);
     return std::min(ni, std::max(nx, 1));
 }
 
@@ -310,7 +347,7 @@ int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, floa
 }
 
 int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
-                 cudaStream_t st, const int* zlimit, int full_first) {
+                 cudaStream_t st, const int* zlimit, int full_first, uint8_t* mask) {
     int steps;
     float dtp, decay;
     int rc = plume_policy_steps(p, &steps, &dtp, &decay);
@@ -323,12 +360,16 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     c.dtp = dtp;
     c.decay = decay;
     const dim3 grid((p->ny + TY - 1) / TY, p->nx);
+    // with full_first the whole grid is masked (the context API's first steps write every voxel)
+    k_plume_mask<<<grid, dim3(TZ, TY), 0, st>>>(p->nx, p->ny, p->nz, F, mask, full_first ? nullptr : zlimit);
+    BD_CHECK_LAUNCH("k_plume_mask");
     const long long total = (long long)steps * n_substeps;
     for (long long s = 0; s < total; ++s) {
         const float* in = (s & 1) ? Cb : Ca;
         float* out = (s & 1) ? Ca : Cb;
         const int full = (full_first && s < 2) ? 1 : 0;
-        k_plume_step<<<grid, dim3(TZ, TY), 0, st>>>(p->nx, p->ny, p->nz, c, in, out, F, zlimit, full);
+        k_plume_step<<<grid, dim3(TZ, TY), 0, st>>>(p->nx, p->ny, p->nz, c, in, out, mask,
+                                                    full ? nullptr : zlimit, full);
     }
     BD_CHECK_LAUNCH("k_plume_step");
     if (in_b) *in_b = (int)(total & 1);
@@ -362,9 +403,17 @@ extern "C" int bd_plume_advance(const BdPlumeParams* p, float* Ca, float* Cb, in
         if (in_b) *in_b = 0;
         return BD_OK;
     }
+    cudaStream_t st = as_stream(stream);
+    uint8_t* mask = nullptr;
+    const size_t nv = (size_t)p->nx * p->ny * p->nz;
+    BD_CUDA(cudaMallocAsync((void**)&mask, nv, st));
     // the context API may hold arbitrary values in non-void voxels: the first two steps write
     // every voxel (one per ping-pong buffer), later steps touch the void domain only
-    return plume_launch(p, Ca, Cb, n_substeps, F, in_b, as_stream(stream), nullptr, 1);
+    int rc = plume_launch(p, Ca, Cb, n_substeps, F, in_b, st, nullptr, 1, mask);
+    cudaError_t e = cudaFreeAsync(mask, st);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_status(e, "bd_plume_advance: cudaFreeAsync");
+    return BD_OK;
 }
 
 extern "C" int bd_plume_steps_per_substep(const BdPlumeParams* p, int* n_steps, float* dt_step) {
