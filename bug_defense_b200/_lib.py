@@ -159,6 +159,8 @@ _SIGNATURES = {
     "bd_mc_destroy": (c_int, [c_void_p]),
     "bd_mc_trace": (c_int, [c_void_p, POINTER(McParams), c_void_p, c_void_p, c_void_p, c_void_p,
                             c_void_p, c_void_p, c_void_p]),
+    "bd_mc_trace_noalloc": (c_int, [POINTER(McParams), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                    c_void_p, c_void_p]),
     "bd_fold_f32_to_f64": (c_int, [c_void_p, c_void_p, c_int64, c_void_p]),
     "bd_thermal_advance": (c_int, [POINTER(ThermalParams), c_void_p, c_void_p, c_int, c_void_p,
                                    c_void_p, c_void_p, c_void_p]),

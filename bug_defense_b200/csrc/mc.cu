@@ -23,6 +23,7 @@
 #include <stdlib.h>
 
 #include <algorithm>
+#include <mutex>
 
 namespace bd {
 
@@ -568,4 +569,70 @@ extern "C" int bd_fold_f32_to_f64(float* src, double* dst, int64_t n, void* stre
     k_fold<<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(src, dst, n);
     BD_CHECK_LAUNCH("k_fold");
     return BD_OK;
+}
+
+// ------------------------------------------------------------------------------------
+// Allocation-free variant of bd_mc_trace.
+//
+// Some callers cannot call cudaMalloc once they are running: a control loop that must keep a
+// fixed latency per laser pulse (the allocator may synchronise the device or block on the
+// driver), or a host framework that owns all device memory through its own pool and does not
+// allow side allocations. bd_mc_trace_noalloc needs no allocation at all: its scratch (the
+// photon-queue counter and one FP64 ledger row per block) is a file-scope device array of fixed
+// size, which every GPU that loads this library holds until the process exits.
+namespace bd {
+constexpr int MC_NOALLOC_MAX_BLOCKS = 2048;
+constexpr size_t MC_NOALLOC_QUEUE_BYTES = 256;
+static __device__ __align__(256) unsigned char g_mc_noalloc_scratch[MC_NOALLOC_QUEUE_BYTES +
+                                                                    sizeof(double) * BD_LEDGER_LEN *
+                                                                        MC_NOALLOC_MAX_BLOCKS];
+constexpr int MC_NOALLOC_MAX_DEVICES = 64;
+static void* g_mc_noalloc_ptr[MC_NOALLOC_MAX_DEVICES] = {nullptr};
+static int g_mc_noalloc_sms[MC_NOALLOC_MAX_DEVICES] = {0};
+static std::mutex g_mc_noalloc_mu;
+}  // namespace bd
+
+extern "C" int bd_mc_trace_noalloc(const BdMcParams* p, const float* props, const uint8_t* flags, float* A,
+                                   float* L, double* lat_depth, double* ledger, void* stream) {
+    int rc = mc_validate(p);
+    if (rc) return rc;
+    BD_REQUIRE(props != nullptr && A != nullptr && ledger != nullptr,
+               "bd_mc_trace_noalloc: props, A and ledger are required");
+    BD_REQUIRE(!(p->options & BD_MC_TALLY_FLUENCE) || L != nullptr, "bd_mc_trace_noalloc: BD_MC_TALLY_FLUENCE needs L");
+    int dev = 0;
+    BD_CUDA(cudaGetDevice(&dev));
+    BD_REQUIRE(dev >= 0 && dev < MC_NOALLOC_MAX_DEVICES, "bd_mc_trace_noalloc: device ordinal %d >= %d", dev,
+               MC_NOALLOC_MAX_DEVICES);
+    void* base = nullptr;
+    int sms = 0;
+    {
+        // set-up once per device, with that device current: the array's name is only a host-side
+        // stand-in, the kernel must be given the device address of this device's copy
+        std::lock_guard<std::mutex> lock(g_mc_noalloc_mu);
+        if (g_mc_noalloc_ptr[dev] == nullptr) {
+            void* ptr = nullptr;
+            BD_CUDA(cudaGetSymbolAddress(&ptr, g_mc_noalloc_scratch));
+            int n = 0;
+            BD_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+            g_mc_noalloc_ptr[dev] = ptr;
+            g_mc_noalloc_sms[dev] = n;
+        }
+        base = g_mc_noalloc_ptr[dev];
+        sms = g_mc_noalloc_sms[dev];
+    }
+    // the grid this launch needs (persistent, occupancy-sized) must fit the static ledger rows
+    int per_sm = 0;
+    if (p->launch_axis == 0) BD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mc_trace<2>, 128, 0));
+    else BD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mc_trace<0>, 128, 0));
+    per_sm = std::max(1, std::min(per_sm, 16));
+    const long long need = std::max(1LL, std::min<long long>((p->n_photons + 127) / 128, (long long)sms * per_sm));
+    if (need > MC_NOALLOC_MAX_BLOCKS)
+        return fail(BD_ERR_INVALID_ARG,
+                    "bd_mc_trace_noalloc: this launch needs %lld blocks but the static scratch holds %d "
+                    "(use bd_mc_trace)", need, MC_NOALLOC_MAX_BLOCKS);
+    unsigned long long* queue = static_cast<unsigned long long*>(base);
+    double* partials = reinterpret_cast<double*>(static_cast<unsigned char*>(base) + MC_NOALLOC_QUEUE_BYTES);
+    // mc_launch zeroes the queue counter and the ledger rows it uses before the kernel runs
+    return mc_launch(p, props, flags, A, L, lat_depth, ledger, queue, partials, MC_NOALLOC_MAX_BLOCKS, sms,
+                     as_stream(stream), nullptr);
 }

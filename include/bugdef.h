@@ -180,6 +180,18 @@ BD_API int bd_mc_destroy(BdMcContext* ctx);
  * trace_photons (voxel_mc_metal.py:508-530) and _mc3d_trace_photons (voxel_mc_3d.py:340-422). */
 BD_API int bd_mc_trace(BdMcContext* ctx, const BdMcParams* p, const float* props, const uint8_t* flags,
                 float* A, float* L, double* lat_depth, double* ledger, void* stream);
+/* bd_mc_trace without any device allocation. No counterpart in the reference: it is for
+ * callers that must not allocate device memory while running -- a fixed-latency control loop
+ * (an allocation can synchronise the device or block in the driver) or a host framework that
+ * owns all device memory through its own pool. Its scratch (photon-queue counter + one FP64
+ * ledger row per block, 256 B + 2048 x 16 doubles = 256.25 KiB) is a static device array that
+ * every GPU loading this library holds until the process exits. The first call on a device
+ * looks up that device's copy of the array, so make it before any timing-critical phase.
+ * Launches needing more than 2048 blocks are rejected with BD_ERR_INVALID_ARG. Every call
+ * shares the array: calls that overlap on the GPU (other streams, other host threads on the
+ * same device) race and must be serialised by the caller. Results equal bd_mc_trace's. */
+BD_API int bd_mc_trace_noalloc(const BdMcParams* p, const float* props, const uint8_t* flags, float* A, float* L,
+                               double* lat_depth, double* ledger, void* stream);
 /* dst64[i] += src32[i]; src32[i] = 0 (folds a batch tally into an FP64 accumulator). */
 BD_API int bd_fold_f32_to_f64(float* src32, double* dst64, int64_t n, void* stream);
 
