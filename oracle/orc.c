@@ -239,20 +239,31 @@ static double fresnel(double n1, double n2, double cos_i, double eq) {
     return 0.5 * (rs * rs + rp * rp);
 }
 
-static void refract(double* u, int axis, double eta) {
-    int a1 = (axis + 1) % 3, a2 = (axis + 2) % 3;
-    double s = u[axis] > 0.0 ? 1.0 : -1.0;
-    u[a1] *= eta; u[a2] *= eta;
-    u[axis] = s * sqrt(fmax(0.0, 1.0 - u[a1] * u[a1] - u[a2] * u[a2]));
+static inline void refract3(double* ux, double* uy, double* uz, int axis, double eta) {
+    if (axis == 0) {
+        double sg = *ux > 0.0 ? 1.0 : -1.0;
+        *uy *= eta; *uz *= eta;
+        *ux = sg * sqrt(fmax(0.0, 1.0 - *uy * *uy - *uz * *uz));
+    } else if (axis == 1) {
+        double sg = *uy > 0.0 ? 1.0 : -1.0;
+        *ux *= eta; *uz *= eta;
+        *uy = sg * sqrt(fmax(0.0, 1.0 - *ux * *ux - *uz * *uz));
+    } else {
+        double sg = *uz > 0.0 ? 1.0 : -1.0;
+        *ux *= eta; *uy *= eta;
+        *uz = sg * sqrt(fmax(0.0, 1.0 - *ux * *ux - *uy * *uy));
+    }
 }
 
 enum { L_SPEC = 1, L_DIFF, L_TRANS, L_LAT, L_ABS, L_ABSV, L_GAIN, L_LOSS, L_TRUNC, L_COL, L_CROSS, L_REFL };
 
+/* One photon packet, voxel_mc_3d.py:123-337 (scalar state, as the reference). */
 static void trace_one(const OrcMcParams* P, int64_t pid, const double* mua, const double* mus, const double* gg,
                       const double* nn, double* A, double* L, double* latz, double* led) {
     const int nx = P->nx, ny = P->ny, nz = P->nz;
-    const int D = P->launch_axis == 0 ? 2 : 0;
+    const int zl = P->launch_axis == 0;  /* 1: depth axis z; 0: depth axis x */
     const double eq = P->metal ? 1e-6 : 1e-9, step_eps = P->metal ? 1e-4 : 1e-9, entry_eps = P->metal ? 1e-6 : 1e-9;
+    const double dx = P->dx, dy = P->dy, dz = P->dz;
     Rng rng;
     rng_init(&rng, P->seed, (uint64_t)(P->offset + pid));
     double u1, u2;
@@ -274,127 +285,146 @@ static void trace_one(const OrcMcParams* P, int64_t pid, const double* mua, cons
         double r = sqrt(-2.0 * log(a)) * P->sigma;
         u1 = r * cos(2.0 * M_PI * b); u2 = r * sin(2.0 * M_PI * b);
     }
-    double pos[3], u[3] = {P->ux0, P->uy0, P->uz0};
-    int iv[3];
-    double st = u1 / P->cos_th_safe;
-    if (D == 2) {
-        pos[0] = P->xc + st * P->cos_ph - u2 * P->sin_ph;
-        pos[1] = P->yc + st * P->sin_ph + u2 * P->cos_ph;
-        pos[2] = 0.0;
-        int out = pos[0] < 0 || pos[0] >= P->lx || pos[1] < 0 || pos[1] >= P->ly;
-        if (!out && P->rmax2 > 0) out = (pos[0] - P->xc) * (pos[0] - P->xc) + (pos[1] - P->yc) * (pos[1] - P->yc) >= P->rmax2;
+    double x, y, z, ux = P->ux0, uy = P->uy0, uz = P->uz0;
+    int ix, iy, iz;
+    const double st = u1 / P->cos_th_safe;
+    if (zl) {
+        x = P->xc + st * P->cos_ph - u2 * P->sin_ph;
+        y = P->yc + st * P->sin_ph + u2 * P->cos_ph;
+        z = 0.0;
+        int out = x < 0 || x >= P->lx || y < 0 || y >= P->ly;
+        if (!out && P->rmax2 > 0) out = (x - P->xc) * (x - P->xc) + (y - P->yc) * (y - P->yc) >= P->rmax2;
         if (out) { led[L_LAT] += 1.0; latz[0] += 1.0; return; }
-        iv[0] = (int)(pos[0] / P->dx); if (iv[0] > nx - 1) iv[0] = nx - 1;
-        iv[1] = (int)(pos[1] / P->dy); if (iv[1] > ny - 1) iv[1] = ny - 1;
-        iv[2] = 0;
+        ix = (int)(x / dx); if (ix > nx - 1) ix = nx - 1;
+        iy = (int)(y / dy); if (iy > ny - 1) iy = ny - 1;
+        iz = 0;
     } else {
-        pos[0] = 0.0;
-        pos[1] = P->yc + st * P->cos_ph - u2 * P->sin_ph;
-        pos[2] = P->zc + st * P->sin_ph + u2 * P->cos_ph;
-        int out = pos[1] < 0 || pos[1] >= P->ly || pos[2] < 0 || pos[2] >= P->lz;
-        if (!out && P->rmax2 > 0) out = (pos[1] - P->yc) * (pos[1] - P->yc) + (pos[2] - P->zc) * (pos[2] - P->zc) >= P->rmax2;
+        x = 0.0;
+        y = P->yc + st * P->cos_ph - u2 * P->sin_ph;
+        z = P->zc + st * P->sin_ph + u2 * P->cos_ph;
+        int out = y < 0 || y >= P->ly || z < 0 || z >= P->lz;
+        if (!out && P->rmax2 > 0) out = (y - P->yc) * (y - P->yc) + (z - P->zc) * (z - P->zc) >= P->rmax2;
         if (out) { led[L_LAT] += 1.0; latz[0] += 1.0; return; }
-        iv[0] = 0;
-        iv[1] = (int)(pos[1] / P->dy); if (iv[1] > ny - 1) iv[1] = ny - 1;
-        iv[2] = (int)(pos[2] / P->dz); if (iv[2] > nz - 1) iv[2] = nz - 1;
+        ix = 0;
+        iy = (int)(y / dy); if (iy > ny - 1) iy = ny - 1;
+        iz = (int)(z / dz); if (iz > nz - 1) iz = nz - 1;
     }
-    const double dd[3] = {P->dx, P->dy, P->dz};
-    const int nd[3] = {nx, ny, nz};
-    size_t c = IDX(iv[0], iv[1], iv[2]);
+    size_t c = IDX(ix, iy, iz);
     double n_in = nn[c];
-    double r0 = fresnel(P->n_amb, n_in, u[D], eq);
+    double r0 = fresnel(P->n_amb, n_in, zl ? uz : ux, eq);
     led[L_SPEC] += r0;
     double w = 1.0 - r0;
     if (w <= 0.0) return;
-    if (fabs(n_in - P->n_amb) > entry_eps) refract(u, D, P->n_amb / n_in);
+    if (fabs(n_in - P->n_amb) > entry_eps) refract3(&ux, &uy, &uz, zl ? 2 : 0, P->n_amb / n_in);
     double tau = -log(fmax(rng_uniform(&rng), 1e-12));
+    /* per-photon counters kept in registers, booked once when the photon ends */
+    double n_col = 0.0, n_cross = 0.0, n_refl = 0.0, absorbed = 0.0;
     for (int64_t ev = 0; ev < P->max_events; ++ev) {
-        c = IDX(iv[0], iv[1], iv[2]);
-        double ma = mua[c], mt = ma + mus[c];
-        double s[3];
-        for (int a = 0; a < 3; ++a) {
-            if (u[a] > 1e-15) s[a] = ((iv[a] + 1) * dd[a] - pos[a]) / u[a];
-            else if (u[a] < -1e-15) s[a] = (iv[a] * dd[a] - pos[a]) / u[a];
-            else s[a] = 1e30;
-        }
-        int ax = (s[0] <= s[1] && s[0] <= s[2]) ? 0 : (s[1] <= s[2] ? 1 : 2);
-        double se = fmax(s[ax], 0.0);
+        c = IDX(ix, iy, iz);
+        const double ma = mua[c], mt = ma + mus[c];
+        double sx, sy, sz;
+        if (ux > 1e-15) sx = ((ix + 1) * dx - x) / ux; else if (ux < -1e-15) sx = (ix * dx - x) / ux; else sx = 1e30;
+        if (uy > 1e-15) sy = ((iy + 1) * dy - y) / uy; else if (uy < -1e-15) sy = (iy * dy - y) / uy; else sy = 1e30;
+        if (uz > 1e-15) sz = ((iz + 1) * dz - z) / uz; else if (uz < -1e-15) sz = (iz * dz - z) / uz; else sz = 1e30;
+        int ax;
+        double se;
+        if (sx <= sy && sx <= sz) { ax = 0; se = sx; }
+        else if (sy <= sz) { ax = 1; se = sy; }
+        else { ax = 2; se = sz; }
+        if (se < 0.0) se = 0.0;
         if (mt > 1e-12 && mt * se >= tau) {
-            led[L_COL] += 1.0;
-            double sc = tau / mt;
+            n_col += 1.0;
+            const double sc = tau / mt;
             if (L) L[c] += w * sc;
-            for (int a = 0; a < 3; ++a) pos[a] += sc * u[a];
+            x += sc * ux; y += sc * uy; z += sc * uz;
             if (P->rmax2 > 0) {
-                double p1 = D == 2 ? pos[0] - P->xc : pos[1] - P->yc, p2 = D == 2 ? pos[1] - P->yc : pos[2] - P->zc;
-                if (p1 * p1 + p2 * p2 >= P->rmax2) { led[L_LAT] += w; latz[iv[D]] += w; return; }
+                double p1 = zl ? x - P->xc : y - P->yc, p2 = zl ? y - P->yc : z - P->zc;
+                if (p1 * p1 + p2 * p2 >= P->rmax2) { led[L_LAT] += w; latz[zl ? iz : ix] += w; goto done; }
             }
-            double dw = w * (ma / mt);
+            const double dw = w * (ma / mt);
             w -= dw;
             A[c] += dw;
-            led[L_ABS] += dw;
+            absorbed += dw;
             if (w < 1e-4) {
                 if (rng_uniform(&rng) < 0.1) { led[L_GAIN] += 9.0 * w; w *= 10.0; }
-                else { led[L_LOSS] += w; return; }
+                else { led[L_LOSS] += w; goto done; }
             }
-            double g = gg[c], xi = rng_uniform(&rng), ct;
+            const double g = gg[c], xi = rng_uniform(&rng);
+            double ct;
             if (fabs(g) < 1e-4) ct = 2.0 * xi - 1.0;
             else {
                 double t = (1.0 - g * g) / (1.0 - g + 2.0 * g * xi);
                 ct = (1.0 + g * g - t * t) / (2.0 * g);
                 ct = fmax(-1.0, fmin(1.0, ct));
             }
-            double sth = sqrt(fmax(0.0, 1.0 - ct * ct));
-            double psi = 2.0 * M_PI * rng_uniform(&rng), cp = cos(psi), sp = sin(psi);
-            double nu[3];
-            if (fabs(u[2]) > 0.99999) {
-                double sz = u[2] > 0 ? 1.0 : -1.0;
-                nu[0] = sth * cp; nu[1] = sth * sp; nu[2] = ct * sz;
+            const double sth = sqrt(fmax(0.0, 1.0 - ct * ct));
+            const double psi = 2.0 * M_PI * rng_uniform(&rng), cp = cos(psi), sp = sin(psi);
+            double nux, nuy, nuz;
+            if (fabs(uz) > 0.99999) {
+                double sgz = uz > 0 ? 1.0 : -1.0;
+                nux = sth * cp; nuy = sth * sp; nuz = ct * sgz;
             } else {
-                double den = sqrt(fmax(1.0 - u[2] * u[2], 1e-12));
-                nu[0] = sth * (u[0] * u[2] * cp - u[1] * sp) / den + u[0] * ct;
-                nu[1] = sth * (u[1] * u[2] * cp + u[0] * sp) / den + u[1] * ct;
-                nu[2] = -sth * cp * den + u[2] * ct;
+                double den = sqrt(fmax(1.0 - uz * uz, 1e-12));
+                nux = sth * (ux * uz * cp - uy * sp) / den + ux * ct;
+                nuy = sth * (uy * uz * cp + ux * sp) / den + uy * ct;
+                nuz = -sth * cp * den + uz * ct;
             }
-            double nm = sqrt(nu[0] * nu[0] + nu[1] * nu[1] + nu[2] * nu[2]);
-            if (nm > 1e-12) for (int a = 0; a < 3; ++a) nu[a] /= nm;
-            u[0] = nu[0]; u[1] = nu[1]; u[2] = nu[2];
+            double nm = sqrt(nux * nux + nuy * nuy + nuz * nuz);
+            if (nm > 1e-12) { nux /= nm; nuy /= nm; nuz /= nm; }
+            ux = nux; uy = nuy; uz = nuz;
             tau = -log(fmax(rng_uniform(&rng), 1e-12));
             continue;
         }
-        led[L_CROSS] += 1.0;
+        n_cross += 1.0;
         tau -= mt * se;
         if (L) L[c] += w * se;
-        for (int a = 0; a < 3; ++a) pos[a] += se * u[a];
-        int jv[3] = {iv[0], iv[1], iv[2]};
-        int sd = u[ax] > 0 ? 1 : -1;
-        jv[ax] += sd;
-        pos[ax] = sd > 0 ? (iv[ax] + 1) * dd[ax] : iv[ax] * dd[ax];
-        if (ax == D) {
-            if (jv[D] < 0) {
-                double r = fresnel(nn[c], P->n_amb, u[D], eq);
-                if (r > 0.0 && rng_uniform(&rng) < r) { u[D] = -u[D]; led[L_REFL] += 1.0; continue; }
+        x += se * ux; y += se * uy; z += se * uz;
+        int jx = ix, jy = iy, jz = iz;
+        double cos_face;
+        if (ax == 0) { int sd = ux > 0 ? 1 : -1; jx += sd; x = sd > 0 ? (ix + 1) * dx : ix * dx; cos_face = ux; }
+        else if (ax == 1) { int sd = uy > 0 ? 1 : -1; jy += sd; y = sd > 0 ? (iy + 1) * dy : iy * dy; cos_face = uy; }
+        else { int sd = uz > 0 ? 1 : -1; jz += sd; z = sd > 0 ? (iz + 1) * dz : iz * dz; cos_face = uz; }
+        const int depth_ax = zl ? 2 : 0;
+        if (ax == depth_ax) {
+            const int jd = zl ? jz : jx, ndp = zl ? nz : nx;
+            if (jd < 0) {
+                double r = fresnel(nn[c], P->n_amb, zl ? uz : ux, eq);
+                if (r > 0.0 && rng_uniform(&rng) < r) {
+                    if (zl) uz = -uz; else ux = -ux;
+                    n_refl += 1.0;
+                    continue;
+                }
                 led[L_DIFF] += w;
-                return;
+                goto done;
             }
-            if (jv[D] >= nd[D]) { led[L_TRANS] += w; return; }
-        } else if (jv[0] < 0 || jv[0] >= nx || jv[1] < 0 || jv[1] >= ny || jv[2] < 0 || jv[2] >= nz) {
-            led[L_LAT] += w; latz[iv[D]] += w;
-            return;
+            if (jd >= ndp) { led[L_TRANS] += w; goto done; }
+        } else if (jx < 0 || jx >= nx || jy < 0 || jy >= ny || jz < 0 || jz >= nz) {
+            led[L_LAT] += w; latz[zl ? iz : ix] += w;
+            goto done;
         }
         if (!P->metal && P->rmax2 > 0) {
-            double p1 = D == 2 ? pos[0] - P->xc : pos[1] - P->yc, p2 = D == 2 ? pos[1] - P->yc : pos[2] - P->zc;
-            if (p1 * p1 + p2 * p2 >= P->rmax2) { led[L_LAT] += w; latz[iv[D]] += w; return; }
+            double p1 = zl ? x - P->xc : y - P->yc, p2 = zl ? y - P->yc : z - P->zc;
+            if (p1 * p1 + p2 * p2 >= P->rmax2) { led[L_LAT] += w; latz[zl ? iz : ix] += w; goto done; }
         }
-        size_t cj = IDX(jv[0], jv[1], jv[2]);
-        double n1 = nn[c], n2 = nn[cj];
+        const size_t cj = IDX(jx, jy, jz);
+        const double n1 = nn[c], n2 = nn[cj];
         if (fabs(n1 - n2) > step_eps) {
-            double r = fresnel(n1, n2, u[ax], eq);
-            if ((!P->metal || r > 0.0) && rng_uniform(&rng) < r) { u[ax] = -u[ax]; led[L_REFL] += 1.0; continue; }
-            refract(u, ax, n1 / n2);
+            double r = fresnel(n1, n2, cos_face, eq);
+            if ((!P->metal || r > 0.0) && rng_uniform(&rng) < r) {
+                if (ax == 0) ux = -ux; else if (ax == 1) uy = -uy; else uz = -uz;
+                n_refl += 1.0;
+                continue;
+            }
+            refract3(&ux, &uy, &uz, ax, n1 / n2);
         }
-        iv[0] = jv[0]; iv[1] = jv[1]; iv[2] = jv[2];
+        ix = jx; iy = jy; iz = jz;
     }
     led[L_TRUNC] += w;
+done:
+    led[L_COL] += n_col;
+    led[L_CROSS] += n_cross;
+    led[L_REFL] += n_refl;
+    led[L_ABS] += absorbed;
 }
 
 /* Parallel driver: photons split into n_chunks batches with private FP64 tallies, reduced at
