@@ -143,7 +143,8 @@ class EpochDiag(Structure):
     _fields_ = [("ledger", c_double * 16), ("epoch", c_double), ("time_s", c_double), ("n_new", c_double),
                 ("n_ablated", c_double), ("gap_open", c_double), ("plume_tau", c_double),
                 ("plume_peak_mu_a", c_double), ("plume_ablated_sum", c_double), ("t_optical_ms", c_double),
-                ("t_thermal_ms", c_double), ("t_epoch_end_ms", c_double)]
+                ("t_thermal_ms", c_double), ("t_epoch_end_ms", c_double), ("n_void", c_double),
+                ("void_zlimit", c_double)]
 
 
 # name -> (restype, argtypes); every entry point of include/bugdef.h

@@ -50,7 +50,7 @@ def build(force: bool = False, verbose: bool = False, extra_flags=(), out: Path 
     srcs = [str(CSRC / s) for s in SOURCES if (CSRC / s).exists()]
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
            "-Xcompiler", "-fvisibility=hidden", "-I", str(ROOT / "include"), "-I", str(CSRC),
-           "--expt-relaxed-constexpr", "-lcuda", *extra_flags, "-o", str(lib) + ".tmp", *srcs]
+           "--expt-relaxed-constexpr", *extra_flags, "-o", str(lib) + ".tmp", *srcs]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     res = subprocess.run(cmd, capture_output=True, text=True)

@@ -379,6 +379,7 @@ class CoupledAblationEngine:
             'mc_energy_closure': closure, 't_optical_s': dg.t_optical_ms * 1e-3, 't_thermal_s': dg.t_thermal_ms * 1e-3,
             'plume_transmission': float(math.exp(-tau)), 'plume_tau': tau, 'plume_peak_mu_a': peak,
             'plume_mean_mu_a': mean, 't_epoch_end_s': dg.t_epoch_end_ms * 1e-3, 'ledger': led,
+            'n_void': int(dg.n_void), 'void_zlimit': int(dg.void_zlimit),
         }
 
     # ---- lazily-read state (host float64 / bool copies) -----------------------------

@@ -106,6 +106,7 @@ __global__ void k_epoch_begin(EngineDyn* dyn, double dt_epoch) {
         dyn->plume_tau_sum = 0.0;
         dyn->plume_abl_sum = 0.0;
         dyn->n_ablated = 0.0;
+        dyn->n_void = 0ull;
         dyn->epoch += 1;
         dyn->t += dt_epoch;
         dyn->t_now = (float)dyn->t;
@@ -121,6 +122,7 @@ __global__ void k_epoch_end_only(EngineDyn* dyn) {
         dyn->plume_tau_sum = 0.0;
         dyn->plume_abl_sum = 0.0;
         dyn->n_ablated = 0.0;
+        dyn->n_void = 0ull;
         dyn->t_now = (float)dyn->t;
     }
 }
@@ -285,7 +287,7 @@ extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void*
         ap.zero_src_in_ablated = 1;
         rc = run_stage(e, laser ? e->g_sub_on : e->g_sub_off, &ap, sizeof(ap), graphs, st, [&](cudaStream_t s) -> int {
             int r = ablation_launch(&ap, d.phase.T, d.T_alt, d.n_substeps, d.phase.H_acc, d.omega, d.phase.chi,
-                                    d.phase.flags, d.A, d.phase.k, d.phase.rho_cp, s);
+                                    d.phase.flags, d.A, d.phase.k, d.phase.rho_cp, s, &e->dyn->err);
             if (r) return r;
             if (d.n_substeps & 1)
                 BD_CUDA(cudaMemcpyAsync(d.phase.T, d.T_alt, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
@@ -298,7 +300,7 @@ extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void*
         rc = run_stage(e, e->g_plume, &d.plume, sizeof(d.plume), graphs, st, [&](cudaStream_t s) -> int {
             int in_b = 0;
             int r = plume_launch(&d.plume, d.phase.plume, d.plume_alt, d.n_substeps, d.phase.flags, &in_b, s,
-                                 &e->dyn->void_zlimit, 0, e->plume_mask);
+                                 &e->dyn->void_zlimit, 0, e->plume_mask, &e->dyn->err);
             if (r) return r;
             if (in_b)
                 BD_CUDA(cudaMemcpyAsync(d.phase.plume, d.plume_alt, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
@@ -374,7 +376,10 @@ extern "C" int bd_engine_read_diag(BdEngine* e, BdEpochDiag* out, void* stream) 
     out->plume_tau = h.plume_tau_sum * (double)e->d.plume.dz;
     out->plume_peak_mu_a = (double)__builtin_bit_cast(float, h.plume_peak_bits);
     out->plume_ablated_sum = h.plume_abl_sum;
+    out->n_void = (double)h.n_void;
+    out->void_zlimit = (double)h.void_zlimit;
     out->t_optical_ms = out->t_thermal_ms = out->t_epoch_end_ms = 0.0;
+    if (h.err) return fail(BD_ERR_TIMEOUT, "bd_engine_read_diag: a bounded device wait timed out");
     if (e->timed) {
         float a = 0, b = 0, c = 0;
         if (cudaEventElapsedTime(&a, e->ev[0], e->ev[1]) == cudaSuccess) out->t_optical_ms = a;

@@ -25,7 +25,8 @@ struct EngineDyn {
     float _pad;
     long long mc_offset;  // photon-stream offset of this epoch's MC
     int void_zlimit;      // 1 + deepest slice holding a void voxel (monotone: ablation is irreversible)
-    int _pad2;
+    int err;              // set by a kernel whose bounded wait timed out
+    unsigned long long n_void;  // voxels in the plume domain after this epoch's update
 };
 
 struct PhaseArgs {
@@ -51,9 +52,9 @@ struct PhaseArgs {
 #define BD_PHASE_INIT 1  // breach check (gap_open) + void/plume/props pass only
 int phase_launch(const PhaseArgs& a, int mode, cudaStream_t st);
 int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, float* H, float* Om, float* Chi,
-                    const uint8_t* F, const float* src, const float* K, const float* R, cudaStream_t st);
+                    const uint8_t* F, const float* src, const float* K, const float* R, cudaStream_t st, int* err);
 int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
-                 cudaStream_t st, const int* zlimit, int full_first, uint8_t* mask);
+                 cudaStream_t st, const int* zlimit, int full_first, uint8_t* mask, int* err);
 int plume_policy_steps(const BdPlumeParams* p, int* n_steps, float* dt_step, float* decay_step);
 int mc_launch(const BdMcParams* p, const float* props, const uint8_t* flags, float* A, float* L, double* latz,
               double* ledger, unsigned long long* queue, double* partials, int max_blocks, int sm_count,

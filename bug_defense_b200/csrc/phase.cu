@@ -145,6 +145,7 @@ __global__ void __launch_bounds__(256) k_void_plume(PhaseArgs a, long long nv) {
     double tau_sum = 0.0, abl_sum = 0.0, abl_cnt = 0.0;
     float peak = 0.0f;
     int kmax = -1;
+    unsigned long long n_void = 0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv;
          i += (long long)gridDim.x * blockDim.x) {
         uint8_t f = a.flags[i];
@@ -153,7 +154,10 @@ __global__ void __launch_bounds__(256) k_void_plume(PhaseArgs a, long long nv) {
         const bool vd = ablated || (gap_open && k >= a.gap_k0 && k < a.gap_k1);
         f = vd ? (uint8_t)(f | BD_FLAG_VOID) : (uint8_t)(f & ~BD_FLAG_VOID);
         a.flags[i] = f;
-        if (vd) kmax = max(kmax, k);
+        if (vd) {
+            kmax = max(kmax, k);
+            ++n_void;
+        }
         float mu_ext = 0.0f;
         if (a.has_plume) {
             float raw = a.plume[i];
@@ -180,6 +184,8 @@ __global__ void __launch_bounds__(256) k_void_plume(PhaseArgs a, long long nv) {
             reinterpret_cast<float4*>(a.props)[i] = make_float4(mt, mt > 0.0f ? ma / mt : 0.0f, gg, a.n[i]);
         }
     }
+    __shared__ unsigned long long shu[8];
+    const unsigned long long nvb = block_sum(n_void, shu);
     double s0 = block_sum(tau_sum, shd);
     double s1 = block_sum(abl_sum, shd);
     double s2 = block_sum(abl_cnt, shd);
@@ -197,6 +203,7 @@ __global__ void __launch_bounds__(256) k_void_plume(PhaseArgs a, long long nv) {
         if (s0 != 0.0) atomicAdd(&a.dyn->plume_tau_sum, s0);
         if (s1 != 0.0) atomicAdd(&a.dyn->plume_abl_sum, s1);
         if (s2 != 0.0) atomicAdd(&a.dyn->n_ablated, s2);
+        if (nvb) atomicAdd(&a.dyn->n_void, nvb);
         // non-negative floats order like their bit patterns
         if (pm > 0.0f) atomicMax(&a.dyn->plume_peak_bits, __float_as_uint(pm));
     }

@@ -15,6 +15,7 @@
 // slowest axis), rotating the x-1 / x / x+1 values of T and k through registers, so each
 // T and k value is fetched from DRAM once per substep; y/z neighbours come from L1.
 #include "common.cuh"
+#include "tma.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -131,6 +132,150 @@ __global__ void __launch_bounds__(TZ * TY) k_substep(Geo g, AblConst c, const fl
     }
 }
 
+// TMA-staged fused substep: same arithmetic as k_substep, but a CTA owns a 32 (z) x 16 (y) tile
+// and marches a chunk of x planes; T and k tiles of each plane (1-voxel y halo, 4-voxel z halo)
+// stream through a 4-stage shared-memory ring filled by the TMA engine, and the per-voxel fields of
+// the next plane (rho_cp, source, flags, H) are fetched into registers one plane ahead.
+constexpr int ST_BZ = 32, ST_BY = 16, ST_PZ = ST_BZ + 8, ST_PY = ST_BY + 2, ST_STAGES = 4;
+constexpr unsigned ST_TILE_BYTES = ST_PZ * ST_PY * sizeof(float);
+constexpr int ST_STRIDE = ((ST_PZ * ST_PY * (int)sizeof(float) + 127) / 128) * 128 / (int)sizeof(float);
+static_assert(ST_STRIDE * sizeof(float) % 128 == 0, "stage stride must keep 128-byte alignment");
+
+template <int MODE, int BC, bool ARR, bool CHAR>
+__global__ void __launch_bounds__(TZ * TY) k_substep_tma(const __grid_constant__ CUtensorMap t_map,
+                                                         const __grid_constant__ CUtensorMap k_map, Geo g,
+                                                         AblConst c, float* __restrict__ Tn,
+                                                         const float* __restrict__ src, const float* __restrict__ R,
+                                                         const uint8_t* __restrict__ F, float* __restrict__ H,
+                                                         float* __restrict__ Om, float* __restrict__ Chi,
+                                                         int xc, int* __restrict__ err) {
+    __shared__ __align__(128) float ringT[ST_STAGES][ST_STRIDE];
+    __shared__ __align__(128) float ringK[ST_STAGES][ST_STRIDE];
+    __shared__ __align__(8) unsigned long long bar[ST_STAGES];
+    const int k0 = blockIdx.x * ST_BZ;
+    const int j0 = blockIdx.y * ST_BY;
+    const int ib = blockIdx.z * xc;
+    const int ie = min(g.nx, ib + xc);
+    if (ib >= ie) return;
+    const int tid = threadIdx.y * TZ + threadIdx.x;
+    if (tid == 0) {
+        for (int q = 0; q < ST_STAGES; ++q) mbar_init(&bar[q], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    const int nplanes = ie - ib + 2;
+    if (tid == 0) {
+        for (int q = 0; q < ST_STAGES && q < nplanes; ++q) {
+            mbar_expect_tx(&bar[q], 2 * ST_TILE_BYTES);
+            tma_load_3d(ringT[q], &t_map, k0 - 4, j0 - 1, ib - 1 + q, &bar[q]);
+            tma_load_3d(ringK[q], &k_map, k0 - 4, j0 - 1, ib - 1 + q, &bar[q]);
+        }
+    }
+    const int plane = g.ny * g.nz;
+    const int k = k0 + threadIdx.x;
+    const int jr[2] = {j0 + (int)threadIdx.y, j0 + (int)threadIdx.y + TY};
+    const bool rowok[2] = {k < g.nz && jr[0] < g.ny, k < g.nz && jr[1] < g.ny};
+    float rho_n[2] = {0.f, 0.f}, q_n[2] = {0.f, 0.f}, h_n[2] = {0.f, 0.f};
+    uint8_t f_n[2] = {0, 0};
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+        if (rowok[r]) {
+            const int idx = ib * plane + jr[r] * g.nz + k;
+            rho_n[r] = __ldg(&R[idx]);
+            if (c.is_active) q_n[r] = __ldg(&src[idx]);
+            if (MODE == 1) { f_n[r] = __ldg(&F[idx]); h_n[r] = H[idx]; }
+        }
+    bool ok = mbar_wait(&bar[0], 0);
+    ok = mbar_wait(&bar[1], 0) && ok;
+    for (int i = ib; i < ie; ++i) {
+        const int q = i - ib + 1;
+        float rho_c[2], q_c[2], h_c[2];
+        uint8_t f_c[2];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) { rho_c[r] = rho_n[r]; q_c[r] = q_n[r]; h_c[r] = h_n[r]; f_c[r] = f_n[r]; }
+        if (i + 1 < ie) {
+#pragma unroll
+            for (int r = 0; r < 2; ++r)
+                if (rowok[r]) {
+                    const int idx = (i + 1) * plane + jr[r] * g.nz + k;
+                    rho_n[r] = __ldg(&R[idx]);
+                    if (c.is_active) q_n[r] = __ldg(&src[idx]);
+                    if (MODE == 1) { f_n[r] = __ldg(&F[idx]); h_n[r] = H[idx]; }
+                }
+        }
+        ok = mbar_wait(&bar[(q + 1) % ST_STAGES], ((q + 1) / ST_STAGES) & 1) && ok;
+        const float* Tm = ringT[(q - 1) % ST_STAGES];
+        const float* Tc_ = ringT[q % ST_STAGES];
+        const float* Tp = ringT[(q + 1) % ST_STAGES];
+        const float* Km = ringK[(q - 1) % ST_STAGES];
+        const float* Kc = ringK[q % ST_STAGES];
+        const float* Kp = ringK[(q + 1) % ST_STAGES];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            if (!rowok[r]) continue;
+            const int j = jr[r];
+            const int jy = j - j0;
+            const int idx = i * plane + j * g.nz + k;
+            const int t = (jy + 1) * ST_PZ + threadIdx.x + 4;
+            const float Tc = Tc_[t], kc = Kc[t];
+            const float fw = (i > 0) ? kface(kc, Km[t]) * (Tm[t] - Tc) * g.idx2 : 0.0f;
+            const float fe = (i + 1 < g.nx) ? kface(kc, Kp[t]) * (Tp[t] - Tc) * g.idx2 : 0.0f;
+            const float fs = (j > 0) ? kface(kc, Kc[t - ST_PZ]) * (Tc_[t - ST_PZ] - Tc) * g.idy2 : 0.0f;
+            const float fn = (j + 1 < g.ny) ? kface(kc, Kc[t + ST_PZ]) * (Tc_[t + ST_PZ] - Tc) * g.idy2 : 0.0f;
+            const float ft = (k > 0) ? kface(kc, Kc[t - 1]) * (Tc_[t - 1] - Tc) * g.idz2 : zwall_flux<BC>(Tc, kc, g);
+            const float fb = (k + 1 < g.nz) ? kface(kc, Kc[t + 1]) * (Tc_[t + 1] - Tc) * g.idz2
+                                            : zwall_flux<BC>(Tc, kc, g);
+            const float div = fw + fe + fs + fn + ft + fb;
+            const float rho = rho_c[r];
+            const float cap = fmaxf(rho, 1e-12f);
+            const uint8_t f = f_c[r];
+            float qv = q_c[r] * c.q_scale;
+            if (MODE == 1 && c.zero_src_in_ablated && (f & BD_FLAG_ABLATED)) qv = 0.0f;
+            if (!c.is_active) qv = 0.0f;
+            float Tt = Tc + __fdividef(g.dt * (div + qv), cap);
+            if (MODE == 1) {
+                const bool abl = (f & BD_FLAG_ABLATED) != 0;
+                const bool dry = (f & BD_FLAG_DRY) != 0;
+                if (abl) {
+                    if (Tt > c.t_void) Tt = c.t_void;
+                } else if (!dry) {
+                    const float h = h_c[r];
+                    if (Tt > c.t_abl) {
+                        H[idx] = h + (Tt - c.t_abl) * rho;
+                        Tt = c.t_abl;
+                    } else if (h > 0.0f) {
+                        const float rel = fminf(h, (c.t_abl - Tt) * rho);
+                        H[idx] = h - rel;
+                        Tt = Tt + rel / rho;
+                    }
+                }
+                if (ARR && !abl) Om[idx] += g.dt * c.arr_A * expf(-c.arr_EaR / (Tt + 273.15f));
+                if (CHAR && dry && !abl) {
+                    const float rate = c.char_A * expf(-c.char_EaR / (Tt + 273.15f));
+                    const float x = Chi[idx];
+                    Chi[idx] = 1.0f - (1.0f - x) * expf(-rate * g.dt);
+                }
+            }
+            Tn[idx] = Tt;
+        }
+        __syncthreads();  // every thread is done with plane i-1's stage
+        if (tid == 0 && q + 3 < nplanes) {
+            const int s = (q + 3) % ST_STAGES;
+            fence_proxy_async_smem();
+            mbar_expect_tx(&bar[s], 2 * ST_TILE_BYTES);
+            tma_load_3d(ringT[s], &t_map, k0 - 4, j0 - 1, i + 3, &bar[s]);
+            tma_load_3d(ringK[s], &k_map, k0 - 4, j0 - 1, i + 3, &bar[s]);
+        }
+    }
+    if (!ok) {
+        atomicExch(err, 1);
+        for (int q = 0; q < ST_STAGES; ++q) {
+            const int last = nplanes - 1 - ((nplanes - 1 - q) % ST_STAGES + ST_STAGES) % ST_STAGES;
+            if (last >= 0) mbar_wait(&bar[q], (last / ST_STAGES) & 1);
+        }
+    }
+}
+
 struct PlumeConst {
     float dxy_x, dxy_y, dz_z;  // D_xy*idx2, D_xy*idy2, D_z*idz2
     float vz_over_dz, dtp, decay;
@@ -211,6 +356,116 @@ __global__ void __launch_bounds__(TZ * TY) k_plume_step(int nx, int ny, int nz, 
     }
 }
 
+// TMA-staged plume step: a CTA owns a 32 (z) x 16 (y) column tile and marches a chunk of x
+// planes. Each plane's tile with a one-voxel y halo and a four-voxel z halo (40 x 18 floats, the
+// z start kept 16-byte aligned) is copied into a 4-stage shared-memory ring by the TMA engine,
+// three planes ahead of the one being computed, so every neighbour read comes from shared
+// memory and no thread waits on a global load chain.
+constexpr int PL_BZ = 32, PL_BY = 16, PL_PZ = PL_BZ + 8, PL_PY = PL_BY + 2, PL_STAGES = 4;
+constexpr unsigned PL_TILE_BYTES = PL_PZ * PL_PY * sizeof(float);
+// each stage starts on a 128-byte boundary (TMA shared-memory destination alignment)
+constexpr int PL_STRIDE = ((PL_PZ * PL_PY * (int)sizeof(float) + 127) / 128) * 128 / (int)sizeof(float);
+static_assert(PL_STRIDE * sizeof(float) % 128 == 0, "stage stride must keep 128-byte alignment");
+static_assert(PL_STRIDE >= PL_PZ * PL_PY, "stage too small");
+
+__global__ void __launch_bounds__(TZ * TY) k_plume_step_tma(const __grid_constant__ CUtensorMap in_map,
+                                                            float* __restrict__ Cn, const uint8_t* __restrict__ M,
+                                                            int nx, int ny, int nz, int xc, PlumeConst c,
+                                                            const int* __restrict__ zlimit, int full_write,
+                                                            int* __restrict__ err) {
+    __shared__ __align__(128) float ring[PL_STAGES][PL_STRIDE];
+    __shared__ __align__(8) unsigned long long bar[PL_STAGES];
+    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
+    const int k0 = blockIdx.x * PL_BZ;
+    const int j0 = blockIdx.y * PL_BY;
+    const int ib = blockIdx.z * xc;
+    const int ie = min(nx, ib + xc);
+    if (k0 >= zl || ib >= ie) return;  // uniform over the CTA
+    const int tid = threadIdx.y * TZ + threadIdx.x;
+    if (tid == 0) {
+        for (int q = 0; q < PL_STAGES; ++q) mbar_init(&bar[q], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    const int nplanes = ie - ib + 2;  // planes ib-1 .. ie; q = plane - (ib - 1)
+    if (tid == 0) {
+        for (int q = 0; q < PL_STAGES && q < nplanes; ++q) {
+            mbar_expect_tx(&bar[q], PL_TILE_BYTES);
+            tma_load_3d(ring[q], &in_map, k0 - 4, j0 - 1, ib - 1 + q, &bar[q]);
+        }
+    }
+    // Folded FTCS weights: C' = decay * (w0 c0 + wx (cw+ce) + wy (cs+cn) + wb cb + wt ct),
+    // the same update as plume.py:73-79 with the products distributed.
+    const float wx = c.dtp * c.dxy_x, wy = c.dtp * c.dxy_y, wb = c.dtp * c.dz_z;
+    const float wt = wb + c.dtp * c.vz_over_dz;
+    const float w0 = 1.0f - 2.0f * (wx + wy + wb) - c.dtp * c.vz_over_dz;
+    const int plane = ny * nz;
+    const int k = k0 + threadIdx.x;
+    const bool kin = k < zl;
+    const int jr0 = j0 + threadIdx.y, jr1 = j0 + threadIdx.y + TY;
+    const bool row0 = kin && jr0 < ny, row1 = kin && jr1 < ny;
+    // the mask bytes of the next plane are fetched one iteration ahead of their use
+    uint8_t m0 = 0, m1 = 0;
+    if (row0) m0 = __ldg(&M[ib * plane + jr0 * nz + k]);
+    if (row1) m1 = __ldg(&M[ib * plane + jr1 * nz + k]);
+    bool ok = mbar_wait(&bar[0], 0);
+    ok = mbar_wait(&bar[1], 0) && ok;
+    for (int i = ib; i < ie; ++i) {
+        const int q = i - ib + 1;
+        uint8_t n0 = 0, n1 = 0;
+        if (i + 1 < ie) {
+            if (row0) n0 = __ldg(&M[(i + 1) * plane + jr0 * nz + k]);
+            if (row1) n1 = __ldg(&M[(i + 1) * plane + jr1 * nz + k]);
+        }
+        ok = mbar_wait(&bar[(q + 1) % PL_STAGES], ((q + 1) / PL_STAGES) & 1) && ok;
+        const float* tm = ring[(q - 1) % PL_STAGES];
+        const float* tc = ring[q % PL_STAGES];
+        const float* tp = ring[(q + 1) % PL_STAGES];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const bool active = r == 0 ? row0 : row1;
+            const uint8_t m = r == 0 ? m0 : m1;
+            if (!active) continue;
+            const int jy = threadIdx.y + r * TY;
+            const int idx = i * plane + (j0 + jy) * nz + k;
+            if (!(m & BD_PM_UPDATE)) {
+                if ((m & BD_PM_VOID) || full_write) Cn[idx] = 0.0f;
+                continue;
+            }
+            const int t = (jy + 1) * PL_PZ + threadIdx.x + 4;
+            const float c0 = tc[t];
+            float cw = tm[t], ce = tp[t], cs = tc[t - PL_PZ], cn = tc[t + PL_PZ], cb = tc[t - 1], ct = tc[t + 1];
+            if ((m & 0x3Fu) != 0x3Fu) {  // a solid neighbour: zero-flux wall, its value is the centre's
+                if (!(m & 0x01)) cw = c0;
+                if (!(m & 0x02)) ce = c0;
+                if (!(m & 0x04)) cs = c0;
+                if (!(m & 0x08)) cn = c0;
+                if (!(m & 0x10)) cb = c0;
+                if (!(m & 0x20)) ct = c0;
+            }
+            const float v = (w0 * c0 + wx * (cw + ce) + wy * (cs + cn) + wb * cb + wt * ct) * c.decay;
+            Cn[idx] = fmaxf(v, 0.0f);
+        }
+        m0 = n0;
+        m1 = n1;
+        __syncthreads();  // every thread is done with plane i-1's stage
+        if (tid == 0 && q + 3 < nplanes) {
+            const int s = (q + 3) % PL_STAGES;
+            fence_proxy_async_smem();
+            mbar_expect_tx(&bar[s], PL_TILE_BYTES);
+            tma_load_3d(ring[s], &in_map, k0 - 4, j0 - 1, i + 3, &bar[s]);
+        }
+    }
+    if (!ok) {
+        atomicExch(err, 1);
+        // drain: give any copy still in flight a bounded chance to land before the CTA exits
+        for (int q = 0; q < PL_STAGES; ++q) {
+            const int last = nplanes - 1 - ((nplanes - 1 - q) % PL_STAGES + PL_STAGES) % PL_STAGES;
+            if (last >= 0) mbar_wait(&bar[q], (last / PL_STAGES) & 1);
+        }
+    }
+}
+
 __global__ void k_pack_flags(const uint8_t* __restrict__ abl, const uint8_t* __restrict__ dry,
                              const uint8_t* __restrict__ vd, long long n, uint8_t* __restrict__ out) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -219,6 +474,41 @@ __global__ void k_pack_flags(const uint8_t* __restrict__ abl, const uint8_t* __r
         uint8_t v = vd ? (vd[i] ? 1 : 0) : a;
         out[i] = (uint8_t)(a * BD_FLAG_ABLATED | d * BD_FLAG_DRY | v * BD_FLAG_VOID);
     }
+}
+
+// cuTensorMapEncodeTiled is a driver-API entry point; it is looked up through the runtime so the
+// library does not link libcuda directly (it loads on machines without a driver, for the ABI checks).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(ptr);
+        cudaGetLastError();
+    }
+    return fn;
+}
+
+bool make_tmap_3d_f32(CUtensorMap* out, const void* base, int nx, int ny, int nz, int bz, int by, int bx) {
+    if (nz % 4 != 0 || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)nz, (cuuint64_t)ny, (cuuint64_t)nx};
+    cuuint64_t strides[2] = {(cuuint64_t)nz * sizeof(float), (cuuint64_t)ny * nz * sizeof(float)};
+    cuuint32_t box[3] = {(cuuint32_t)bz, (cuuint32_t)by, (cuuint32_t)bx};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
 }
 
 static dim3 tile_grid(int nx, int ny, int nz, int ni) {
@@ -248,10 +538,31 @@ static Geo make_geo(int nx, int ny, int nz, float dx, float dy, float dz, float 
     return g;
 }
 
+#ifndef BD_STENCIL_XC
+#define BD_STENCIL_XC 8
+#endif
+
 template <int MODE, int BC, bool ARR, bool CHAR>
 static void launch_substeps(const Geo& g, const AblConst& c, float* Ta, float* Tb, int n, const float* src,
                             const float* K, const float* R, const uint8_t* F, float* H, float* Om, float* Chi,
-                            cudaStream_t st) {
+                            cudaStream_t st, int* err) {
+    CUtensorMap ma, mb, mk;
+#ifdef BD_NO_TMA
+    err = nullptr;
+#endif
+    const bool tma = err != nullptr && make_tmap_3d_f32(&ma, Ta, g.nx, g.ny, g.nz, ST_PZ, ST_PY, 1) &&
+                     make_tmap_3d_f32(&mb, Tb, g.nx, g.ny, g.nz, ST_PZ, ST_PY, 1) &&
+                     make_tmap_3d_f32(&mk, K, g.nx, g.ny, g.nz, ST_PZ, ST_PY, 1);
+    if (tma) {
+        const int xc = BD_STENCIL_XC;
+        const dim3 grid((g.nz + ST_BZ - 1) / ST_BZ, (g.ny + ST_BY - 1) / ST_BY, (g.nx + xc - 1) / xc);
+        for (int s = 0; s < n; ++s) {
+            float* out = (s & 1) ? Ta : Tb;
+            k_substep_tma<MODE, BC, ARR, CHAR><<<grid, dim3(TZ, TY), 0, st>>>((s & 1) ? mb : ma, mk, g, c, out, src,
+                                                                             R, F, H, Om, Chi, xc, err);
+        }
+        return;
+    }
     dim3 grid = tile_grid(g.nx, g.ny, g.nz, g.ni), block(TZ, TY);
     for (int s = 0; s < n; ++s) {
         const float* in = (s & 1) ? Tb : Ta;
@@ -292,6 +603,26 @@ int plume_policy_steps(const BdPlumeParams* p, int* n_steps, float* dt_step, flo
     return BD_OK;
 }
 
+// Runs `launch(err)` with a 4-byte device error flag, then synchronises the stream and turns a
+// raised flag (a bounded TMA wait that timed out) into BD_ERR_TIMEOUT.
+template <typename F>
+static int with_error_flag(cudaStream_t st, const char* what, F launch) {
+    int* err = nullptr;
+    BD_CUDA(cudaMallocAsync((void**)&err, sizeof(int), st));
+    int rc = BD_OK;
+    int host_err = 0;
+    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), st);
+    if (e == cudaSuccess) rc = launch(err);
+    if (e == cudaSuccess && rc == BD_OK) e = cudaMemcpyAsync(&host_err, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaError_t e2 = cudaFreeAsync(err, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_status(e, what);
+    if (e2 != cudaSuccess) return cuda_status(e2, what);
+    if (host_err) return fail(BD_ERR_TIMEOUT, "%s: a bounded TMA wait timed out", what);
+    return BD_OK;
+}
+
 }  // namespace bd
 
 using namespace bd;
@@ -311,17 +642,21 @@ extern "C" int bd_thermal_advance(const BdThermalParams* p, float* Ta, float* Tb
     c.q_scale = p->q_scale;
     c.is_active = p->is_active;
     cudaStream_t st = as_stream(stream);
-    if (p->bc_mode == BD_BC_SERIES)
-        launch_substeps<0, BD_BC_SERIES, false, false>(g, c, Ta, Tb, n, src, K, R, nullptr, nullptr, nullptr, nullptr, st);
-    else
-        launch_substeps<0, BD_BC_METAL, false, false>(g, c, Ta, Tb, n, src, K, R, nullptr, nullptr, nullptr, nullptr, st);
-    BD_CHECK_LAUNCH("k_substep<thermal>");
-    return BD_OK;
+    return with_error_flag(st, "bd_thermal_advance", [&](int* err) -> int {
+        if (p->bc_mode == BD_BC_SERIES)
+            launch_substeps<0, BD_BC_SERIES, false, false>(g, c, Ta, Tb, n, src, K, R, nullptr, nullptr, nullptr,
+                                                           nullptr, st, err);
+        else
+            launch_substeps<0, BD_BC_METAL, false, false>(g, c, Ta, Tb, n, src, K, R, nullptr, nullptr, nullptr,
+                                                          nullptr, st, err);
+        BD_CHECK_LAUNCH("k_substep<thermal>");
+        return BD_OK;
+    });
 }
 
 namespace bd {
 int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, float* H, float* Om, float* Chi,
-                    const uint8_t* F, const float* src, const float* K, const float* R, cudaStream_t st) {
+                    const uint8_t* F, const float* src, const float* K, const float* R, cudaStream_t st, int* err) {
     Geo g = make_geo(p->nx, p->ny, p->nz, p->dx, p->dy, p->dz, p->dt, p->h_eff, p->t_ambient);
     AblConst c;
     c.t_abl = p->t_abl; c.t_void = p->t_void; c.q_scale = p->q_scale;
@@ -330,7 +665,7 @@ int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, floa
     const bool arr = p->has_arrhenius != 0, chr = p->has_char != 0;
 #define BD_ABL_CASE(BCV, A_, C_)                                                                 \
     if (p->bc_mode == BCV && arr == A_ && chr == C_) {                                           \
-        launch_substeps<1, BCV, A_, C_>(g, c, Ta, Tb, n, src, K, R, F, H, Om, Chi, st);          \
+        launch_substeps<1, BCV, A_, C_>(g, c, Ta, Tb, n, src, K, R, F, H, Om, Chi, st, err);     \
         BD_CHECK_LAUNCH("k_substep<ablation>");                                                  \
         return BD_OK;                                                                            \
     }
@@ -346,8 +681,12 @@ int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, floa
     return fail(BD_ERR_INVALID_ARG, "bd_ablation_advance: bad bc_mode %d", p->bc_mode);
 }
 
+#ifndef BD_PLUME_XC
+#define BD_PLUME_XC 8
+#endif
+
 int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
-                 cudaStream_t st, const int* zlimit, int full_first, uint8_t* mask) {
+                 cudaStream_t st, const int* zlimit, int full_first, uint8_t* mask, int* err) {
     int steps;
     float dtp, decay;
     int rc = plume_policy_steps(p, &steps, &dtp, &decay);
@@ -363,13 +702,25 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     // with full_first the whole grid is masked (the context API's first steps write every voxel)
     k_plume_mask<<<grid, dim3(TZ, TY), 0, st>>>(p->nx, p->ny, p->nz, F, mask, full_first ? nullptr : zlimit);
     BD_CHECK_LAUNCH("k_plume_mask");
+    CUtensorMap map_a, map_b;
+#ifdef BD_NO_TMA
+    err = nullptr;
+#endif
+    const bool tma = err != nullptr && make_tmap_3d_f32(&map_a, Ca, p->nx, p->ny, p->nz, PL_PZ, PL_PY, 1) &&
+                     make_tmap_3d_f32(&map_b, Cb, p->nx, p->ny, p->nz, PL_PZ, PL_PY, 1);
+    const int xc = BD_PLUME_XC;
+    const dim3 tgrid((p->nz + PL_BZ - 1) / PL_BZ, (p->ny + PL_BY - 1) / PL_BY, (p->nx + xc - 1) / xc);
     const long long total = (long long)steps * n_substeps;
     for (long long s = 0; s < total; ++s) {
         const float* in = (s & 1) ? Cb : Ca;
         float* out = (s & 1) ? Ca : Cb;
         const int full = (full_first && s < 2) ? 1 : 0;
-        k_plume_step<<<grid, dim3(TZ, TY), 0, st>>>(p->nx, p->ny, p->nz, c, in, out, mask,
-                                                    full ? nullptr : zlimit, full);
+        if (tma)
+            k_plume_step_tma<<<tgrid, dim3(TZ, TY), 0, st>>>((s & 1) ? map_b : map_a, out, mask, p->nx, p->ny, p->nz,
+                                                             xc, c, full ? nullptr : zlimit, full, err);
+        else
+            k_plume_step<<<grid, dim3(TZ, TY), 0, st>>>(p->nx, p->ny, p->nz, c, in, out, mask,
+                                                        full ? nullptr : zlimit, full);
     }
     BD_CHECK_LAUNCH("k_plume_step");
     if (in_b) *in_b = (int)(total & 1);
@@ -389,7 +740,10 @@ extern "C" int bd_ablation_advance(const BdAblationParams* p, float* Ta, float* 
     BD_REQUIRE(n >= 0, "bd_ablation_advance: n_substeps must be >= 0");
     BD_REQUIRE((long long)p->nx * p->ny * p->nz < (1LL << 31), "bd_ablation_advance: grid exceeds 2^31 voxels");
     if (n == 0) return BD_OK;
-    return ablation_launch(p, Ta, Tb, n, H, Om, Chi, F, src, K, R, as_stream(stream));
+    cudaStream_t st = as_stream(stream);
+    return with_error_flag(st, "bd_ablation_advance", [&](int* err) -> int {
+        return ablation_launch(p, Ta, Tb, n, H, Om, Chi, F, src, K, R, st, err);
+    });
 }
 
 extern "C" int bd_plume_advance(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F,
@@ -404,15 +758,24 @@ extern "C" int bd_plume_advance(const BdPlumeParams* p, float* Ca, float* Cb, in
         return BD_OK;
     }
     cudaStream_t st = as_stream(stream);
-    uint8_t* mask = nullptr;
     const size_t nv = (size_t)p->nx * p->ny * p->nz;
-    BD_CUDA(cudaMallocAsync((void**)&mask, nv, st));
+    unsigned char* scratch = nullptr;  // plume neighbourhood bytes + a 4-byte error flag
+    const size_t flag_off = (nv + 15) & ~(size_t)15;
+    BD_CUDA(cudaMallocAsync((void**)&scratch, flag_off + 16, st));
+    int* err = reinterpret_cast<int*>(scratch + flag_off);
+    int rc = BD_OK;
+    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), st);
     // the context API may hold arbitrary values in non-void voxels: the first two steps write
     // every voxel (one per ping-pong buffer), later steps touch the void domain only
-    int rc = plume_launch(p, Ca, Cb, n_substeps, F, in_b, st, nullptr, 1, mask);
-    cudaError_t e = cudaFreeAsync(mask, st);
+    if (e == cudaSuccess) rc = plume_launch(p, Ca, Cb, n_substeps, F, in_b, st, nullptr, 1, scratch, err);
+    int host_err = 0;
+    if (e == cudaSuccess && rc == BD_OK) e = cudaMemcpyAsync(&host_err, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaError_t e2 = cudaFreeAsync(scratch, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (rc) return rc;
-    if (e != cudaSuccess) return cuda_status(e, "bd_plume_advance: cudaFreeAsync");
+    if (e != cudaSuccess) return cuda_status(e, "bd_plume_advance");
+    if (e2 != cudaSuccess) return cuda_status(e2, "bd_plume_advance: cudaFreeAsync");
+    if (host_err) return fail(BD_ERR_TIMEOUT, "bd_plume_advance: a TMA wait timed out");
     return BD_OK;
 }
 

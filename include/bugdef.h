@@ -279,6 +279,8 @@ typedef struct BdEpochDiag {
     double plume_peak_mu_a;
     double plume_ablated_sum;      /* sum of plume mu_a over ablated voxels                */
     double t_optical_ms, t_thermal_ms, t_epoch_end_ms;  /* device time of the three stages */
+    double n_void;                 /* voxels in the plume domain after this epoch           */
+    double void_zlimit;            /* 1 + deepest slice holding a void voxel                 */
 } BdEpochDiag;
 
 #define BD_EPOCH_SKIP_MC 0x1       /* use the absorbed map already in A (no MC this epoch) */

@@ -185,3 +185,45 @@ def test_phase_update_matches_reference(gpu, golden, name):
         scale = max(np.max(np.abs(g[k_out])), np.max(np.abs(ins[k_in])))
         ok = np.isclose(got, g[k_out], rtol=2e-6, atol=4e-7 * scale) | near
         assert np.all(ok), (k_in, np.max(np.abs(got - g[k_out])))
+
+
+@pytest.mark.parametrize("shape", [(20, 18, 24), (9, 35, 68)])
+def test_plume_tma_path_matches_oracle(gpu, orc, shape):
+    """Grids with nz % 4 == 0 take the TMA-staged plume kernel; compare with the FP64 oracle
+    (itself pinned to the reference plume step) over 15 steps with drift and decay."""
+    rng = np.random.default_rng(sum(shape))
+    Nx, Ny, Nz = shape
+    vd = rng.uniform(size=shape) < 0.8
+    C0 = (rng.uniform(0, 1, shape) * vd).astype(np.float32)
+    dx, dy, dz, dt, Dxy, Dz, vz, tau = 0.03, 0.025, 0.02, 1e-5, 1.5, 2.5, 4.0, 0.02
+    ctx = gpu.MetalAblationContext(Nx, Ny, Nz, dx, dy, dz, dt, 0.0, 20.0, 100.0, 300.0,
+                                   plume_params={'D_xy': Dxy, 'D_z': Dz, 'vz': vz, 'tau_linger': tau},
+                                   plume_dt_policy='as_given')
+    z = np.zeros(shape)
+    ctx.set_state(np.full(shape, 20.0), z, z, z, np.zeros(shape, np.uint8), np.zeros(shape, np.uint8), z, z,
+                  np.full(shape, 1e-3), plume=C0, plume_void=vd)
+    ctx.advance_substeps(15, is_active=0)
+    got = ctx.get_plume()
+    C = C0.astype(np.float64); Cn = np.empty_like(C)
+    decay = float(np.exp(-dt / tau))
+    for _ in range(15):
+        orc.diffuse_plume_step(C, Cn, vd, Nx, Ny, Nz, dx, dy, dz, dt, Dxy, Dz, vz, decay)
+        C, Cn = Cn, C
+    np.testing.assert_allclose(got, C, rtol=1e-4, atol=1e-6)
+    assert np.all(got[~vd] == 0.0)
+
+
+@pytest.mark.parametrize("shape", [(20, 18, 24), (7, 33, 64)])
+def test_thermal_tma_path_matches_oracle(gpu, orc, shape):
+    """Grids with nz % 4 == 0 take the TMA-staged stencil; compare with the FP64 oracle over 12 steps."""
+    rng = np.random.default_rng(7 + sum(shape))
+    Nx, Ny, Nz = shape
+    T0 = rng.uniform(20, 120, shape); Q = rng.uniform(0, 900, shape)
+    k = rng.uniform(2e-4, 6e-4, shape); rho = rng.uniform(1.5e-3, 4e-3, shape)
+    dx, dy, dz, dt, h, ta = 0.03, 0.025, 0.02, 2e-5, 15e-6, 20.0
+    got = gpu.run_thermal3d_substeps_gpu(T0, Q, k, rho, Nx, Ny, Nz, dx, dy, dz, dt, 12, h, ta, 1)
+    T, Tn = T0.copy(), np.empty_like(T0)
+    for _ in range(12):
+        orc.thermal3d_step_explicit(T, Tn, Q, k, rho, Nx, Ny, Nz, dx, dy, dz, dt, h, ta, 1)
+        T, Tn = Tn, T
+    assert np.max(np.abs(got - T) / np.abs(T)) <= 1e-5
