@@ -423,28 +423,23 @@ __global__ void __launch_bounds__(TZ * TY) k_plume_step_tma(const __grid_constan
         const float* tp = ring[(q + 1) % PL_STAGES];
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
+            // branch-free: every lane evaluates the stencil (its tile indices are always inside the
+            // shared-memory stage), the mask byte selects neighbours and the result, and a single
+            // predicated store writes void voxels only
             const bool active = r == 0 ? row0 : row1;
             const uint8_t m = r == 0 ? m0 : m1;
-            if (!active) continue;
             const int jy = threadIdx.y + r * TY;
-            const int idx = i * plane + (j0 + jy) * nz + k;
-            if (!(m & BD_PM_UPDATE)) {
-                if ((m & BD_PM_VOID) || full_write) Cn[idx] = 0.0f;
-                continue;
-            }
             const int t = (jy + 1) * PL_PZ + threadIdx.x + 4;
             const float c0 = tc[t];
-            float cw = tm[t], ce = tp[t], cs = tc[t - PL_PZ], cn = tc[t + PL_PZ], cb = tc[t - 1], ct = tc[t + 1];
-            if ((m & 0x3Fu) != 0x3Fu) {  // a solid neighbour: zero-flux wall, its value is the centre's
-                if (!(m & 0x01)) cw = c0;
-                if (!(m & 0x02)) ce = c0;
-                if (!(m & 0x04)) cs = c0;
-                if (!(m & 0x08)) cn = c0;
-                if (!(m & 0x10)) cb = c0;
-                if (!(m & 0x20)) ct = c0;
-            }
-            const float v = (w0 * c0 + wx * (cw + ce) + wy * (cs + cn) + wb * cb + wt * ct) * c.decay;
-            Cn[idx] = fmaxf(v, 0.0f);
+            const float w = (m & 0x01) ? tm[t] : c0;
+            const float e = (m & 0x02) ? tp[t] : c0;
+            const float sx = (m & 0x04) ? tc[t - PL_PZ] : c0;
+            const float nn = (m & 0x08) ? tc[t + PL_PZ] : c0;
+            const float b = (m & 0x10) ? tc[t - 1] : c0;
+            const float tt = (m & 0x20) ? tc[t + 1] : c0;
+            float v = fmaxf((w0 * c0 + wx * (w + e) + wy * (sx + nn) + wb * b + wt * tt) * c.decay, 0.0f);
+            v = (m & BD_PM_UPDATE) ? v : 0.0f;
+            if (active && ((m & BD_PM_VOID) || full_write)) Cn[i * plane + (j0 + jy) * nz + k] = v;
         }
         m0 = n0;
         m1 = n1;
@@ -682,7 +677,7 @@ int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, floa
 }
 
 #ifndef BD_PLUME_XC
-#define BD_PLUME_XC 8
+#define BD_PLUME_XC 4
 #endif
 
 int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
