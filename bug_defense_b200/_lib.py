@@ -147,6 +147,24 @@ class EpochDiag(Structure):
                 ("void_zlimit", c_double)]
 
 
+CONV_FWD_RELU = 0
+CONV_FWD_UPADD = 1
+CONV_FWD_HEAD = 2
+CONV_BWD_RAW = 3
+CONV_BWD_MASK = 4
+CONV_BWD_UPADD = 5
+
+
+class ConvCall(Structure):
+    _fields_ = [
+        ("nx", c_int32), ("ny", c_int32), ("nz", c_int32), ("cin", c_int32), ("cout_total", c_int32),
+        ("n_off", c_int32), ("n_slice", c_int32), ("taps", c_int32), ("mode", c_int32),
+        ("input", _F), ("wimage", _F), ("bias", _F), ("out", _F), ("out_coarse", _F), ("aux", _F), ("aux2", _F),
+        ("head", _F), ("a_noisy", _F), ("mask", _F), ("scale", c_float), ("loss_norm", c_float),
+        ("pred", _F), ("target", _F), ("head_grad", _F), ("loss", _F), ("grad_out", _F),
+    ]
+
+
 # name -> (restype, argtypes); every entry point of include/bugdef.h
 _SIGNATURES = {
     "bd_abi_version": (c_int, []),
@@ -180,6 +198,22 @@ _SIGNATURES = {
     "bd_engine_set_mc": (c_int, [c_void_p, POINTER(McParams)]),
     "bd_engine_timing": (c_int, [c_void_p, c_int]),
     "bd_engine_timing_read": (c_int, [c_void_p, POINTER(c_double), POINTER(c_int64)]),
+    "bd_conv_image_bytes": (c_int64, [c_int, c_int, c_int]),
+    "bd_conv_pack_weights": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    "bd_conv3d": (c_int, [POINTER(ConvCall), c_void_p]),
+    "bd_conv3d_wgrad": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p,
+                                c_void_p]),
+    "bd_unet_param_count": (c_int64, []),
+    "bd_unet_create": (c_int, [c_int, c_int, c_int, c_int, POINTER(c_void_p)]),
+    "bd_unet_destroy": (c_int, [c_void_p]),
+    "bd_unet_set_params": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "bd_unet_get_params": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "bd_unet_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_float, c_void_p, c_void_p]),
+    "bd_unet_forward_backward": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_float, c_float,
+                                         c_void_p, c_void_p]),
+    "bd_unet_get_grads": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "bd_unet_adam": (c_int, [c_void_p, c_float, c_float, c_float, c_float, c_void_p]),
+    "bd_unet_read_loss": (c_int, [c_void_p, POINTER(c_double), c_void_p]),
 }
 
 _lib = None

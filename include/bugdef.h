@@ -313,6 +313,89 @@ BD_API int bd_engine_set_mc(BdEngine* e, const BdMcParams* mc);
 BD_API int bd_engine_timing(BdEngine* e, int enable);
 BD_API int bd_engine_timing_read(BdEngine* e, double* stage_ms /* [4] */, int64_t* epochs);
 
+/* ---------------------------------------------------------------------------------------------
+ * Absorbed-map denoiser: 3-D convolution layers (tcgen05 BF16 tensor cores, FP32 accumulation).
+ * No counterpart in the reference, which has no learned component; these are the building blocks
+ * of the U-Net that denoises low-photon absorbed-power maps.
+ *
+ * Volumes are channels-last bf16 with a one-voxel zero pad: a level with interior nx x ny x nz
+ * stores (nx+2)(ny+2)(nz+2) rows of `channels` values, z fastest, and every call keeps the pad
+ * rows zero. Taps are ordered t = (dx+1)*9 + (dy+1)*3 + (dz+1) (27 taps) or t = (dx+1)*3 + (dy+1)
+ * (9 taps, for an input whose z neighbours are packed into its channels); weights are FP32
+ * [taps][cout][cin]. */
+#define BD_CONV_FWD_RELU   0  /* out = relu(conv + bias) at this level                               */
+#define BD_CONV_FWD_UPADD  1  /* out(finer) = up2(relu(conv + bias)) + aux(finer); out_coarse = relu  */
+#define BD_CONV_FWD_HEAD   2  /* 1x1 head + residual on the noisy map, loss and head gradient fused  */
+#define BD_CONV_BWD_RAW    3  /* out = conv (transposed weights)                                     */
+#define BD_CONV_BWD_MASK   4  /* out = conv * (aux > 0)                                              */
+#define BD_CONV_BWD_UPADD  5  /* out(finer) = (aux(finer) + up2(conv)/8) * (aux2(finer) > 0)         */
+
+typedef struct BdConvCall {
+    int nx, ny, nz;          /* interior size of the level the convolution runs on                  */
+    int cin;                 /* channels per input row (16, 32 or 64)                               */
+    int cout_total;          /* channels per output row                                             */
+    int n_off, n_slice;      /* output channels [n_off, n_off + n_slice) computed by this call      */
+    int taps;                /* 27 or 9                                                             */
+    int mode;                /* BD_CONV_*                                                           */
+    const void* input;       /* bf16 padded input rows                                              */
+    const void* wimage;      /* weight image of this slice (bd_conv_pack_weights)                   */
+    const float* bias;       /* [n_slice] (forward modes) or NULL                                   */
+    void* out;               /* bf16 padded output rows (finer level for the UPADD modes)           */
+    void* out_coarse;        /* FWD_UPADD: optional copy of relu(conv + bias) at this level         */
+    const void* aux;         /* see the modes above                                                 */
+    const void* aux2;
+    /* FWD_HEAD only (n_slice == cout_total == 16): pred = (a_noisy*scale + head.relu(conv+bias)) *
+     * mask, written unpadded as pred/scale; with a target, loss += sum (pred - target*scale)^2 and
+     * grad_out / head_grad receive the gradients of loss * loss_norm. */
+    const float* head;       /* [17] weights then bias                                              */
+    const float* a_noisy;    /* fp32 [nx*ny*nz]                                                     */
+    const uint8_t* mask;     /* [nx*ny*nz] 0 or 1                                                   */
+    float scale;
+    float loss_norm;
+    float* pred;             /* fp32 [nx*ny*nz]                                                     */
+    const float* target;     /* fp32 [nx*ny*nz] or NULL (inference)                                 */
+    float* head_grad;        /* [17], accumulated                                                   */
+    double* loss;            /* [1], accumulated                                                    */
+    void* grad_out;          /* bf16 padded [.][16] gradient at the head input                      */
+} BdConvCall;
+
+/* Bytes of the shared-memory weight image of one output-channel slice. */
+BD_API int64_t bd_conv_image_bytes(int taps, int k_channels, int n_slice);
+/* FP32 [taps][cout][cin] -> bf16 image for output channels [n_off, n_off + n_slice). transpose=0:
+ * the forward convolution (K = cin); transpose=1: the data-gradient convolution, whose outputs are
+ * the layer's input channels (K = cout, taps mirrored). */
+BD_API int bd_conv_pack_weights(int taps, int cin, int cout, int n_off, int n_slice, int transpose,
+                                const float* w, void* wimage, void* stream);
+BD_API int bd_conv3d(const BdConvCall* c, void* stream);
+/* dw[t][co][ci] += sum over voxels of grad[v][co] * act[v + offset(t)][ci] (FP32 atomics). */
+BD_API int bd_conv3d_wgrad(int nx, int ny, int nz, int cin, int cout, int taps, const void* grad,
+                           const void* act, float* dw, void* stream);
+
+/* The denoiser network (3-level U-Net, 16/32/64 channels) over an nx x ny x nz MC grid (multiples
+ * of 4). Inputs: the noisy absorbed map (fraction of launched weight per voxel, as bd_mc_trace
+ * tallies it), the packed MC properties (bd_mc_pack_props: mu_t, mu_a/mu_t, g, n per voxel) and the
+ * optional flag bytes; `scale` multiplies the map into the network's working range. Parameters are
+ * one FP32 vector of bd_unet_param_count() values: per layer W[taps][cout][cin] then b[cout], the
+ * layers (taps, cin, cout) = (9,16,16) (27,16,16) (27,16,32) (27,32,32) (27,32,64) (27,64,64)
+ * (27,64,32) (27,32,32) (27,32,16) (27,16,16), then 16 head weights and the head bias. */
+typedef struct BdUnet BdUnet;
+BD_API int64_t bd_unet_param_count(void);
+BD_API int bd_unet_create(int nx, int ny, int nz, int training, BdUnet** out);
+BD_API int bd_unet_destroy(BdUnet* net);
+BD_API int bd_unet_set_params(BdUnet* net, const float* params, void* stream);   /* resets Adam state */
+BD_API int bd_unet_get_params(BdUnet* net, float* params, void* stream);
+BD_API int bd_unet_forward(BdUnet* net, const float* a_noisy, const float* props, const uint8_t* flags,
+                           float scale, float* pred, void* stream);
+/* Training pass: forward, loss = sum (pred - target)^2 * scale^2 over absorbing voxels, and the
+ * gradient of loss * loss_norm into the network's gradient vector. */
+BD_API int bd_unet_forward_backward(BdUnet* net, const float* a_noisy, const float* props,
+                                    const uint8_t* flags, const float* target, float scale,
+                                    float loss_norm, float* pred, void* stream);
+BD_API int bd_unet_get_grads(BdUnet* net, float* grads, void* stream);
+BD_API int bd_unet_adam(BdUnet* net, float lr, float beta1, float beta2, float eps, void* stream);
+/* Synchronises `stream`; returns the last training loss and BD_ERR_TIMEOUT if a kernel gave up. */
+BD_API int bd_unet_read_loss(BdUnet* net, double* loss, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,7 +13,7 @@ HEADER = ROOT / "include" / "bugdef.h"
 
 
 def declared():
-    return re.findall(r"BD_API\s+int\s+(bd_\w+)\s*\(", HEADER.read_text())
+    return re.findall(r"BD_API\s+\w+\s+(bd_\w+)\s*\(", HEADER.read_text())
 
 
 @pytest.fixture(scope="module")
@@ -53,10 +53,10 @@ def test_version_and_errors_without_gpu(lib):
 
 
 STRUCTS = ["BdMcParams", "BdThermalParams", "BdAblationParams", "BdPlumeParams", "BdGridRef", "BdPhaseDesc",
-           "BdEngineDesc", "BdEpochDiag"]
+           "BdEngineDesc", "BdEpochDiag", "BdConvCall"]
 PY = {"BdMcParams": "McParams", "BdThermalParams": "ThermalParams", "BdAblationParams": "AblationParams",
       "BdPlumeParams": "PlumeParams", "BdGridRef": "GridRef", "BdPhaseDesc": "PhaseDesc",
-      "BdEngineDesc": "EngineDesc", "BdEpochDiag": "EpochDiag"}
+      "BdEngineDesc": "EngineDesc", "BdEpochDiag": "EpochDiag", "BdConvCall": "ConvCall"}
 
 
 def test_struct_layouts_match_header():
