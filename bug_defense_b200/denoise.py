@@ -86,3 +86,95 @@ def conv3d_wgrad(grad, act, dw, shape, cin, cout, taps=27, stream=None):
     nx, ny, nz = shape
     _lib.call("bd_conv3d_wgrad", nx, ny, nz, cin, cout, taps, _lib.ptr(grad), _lib.ptr(act), _lib.ptr(dw),
               _lib.stream_ptr(stream))
+
+
+class UNet:
+    """Device-resident denoiser network (bd_unet_*): parameters, activations and, with
+    training=True, gradients and Adam moments, for one grid shape (multiples of 4)."""
+
+    def __init__(self, shape, training: bool = False, params=None, device=None):
+        torch = _torch()
+        self.shape = tuple(int(s) for s in shape)
+        self.training = bool(training)
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _lib.call("bd_unet_create", *self.shape, int(self.training), ctypes.byref(h))
+        self._h = h
+        self.n_params = int(_lib.load().bd_unet_param_count())
+        assert self.n_params == N_PARAMS
+        if params is not None:
+            self.set_params(params)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.load().bd_unet_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params, stream=None):
+        torch = _torch()
+        p = torch.as_tensor(params, dtype=torch.float32).to(self.device).contiguous()
+        if p.numel() != self.n_params:
+            raise ValueError(f"expected {self.n_params} parameters, got {p.numel()}")
+        self._staged = p
+        _lib.call("bd_unet_set_params", self._h, _lib.ptr(p), _lib.stream_ptr(stream))
+
+    def params(self, stream=None):
+        torch = _torch()
+        out = torch.empty(self.n_params, dtype=torch.float32, device=self.device)
+        _lib.call("bd_unet_get_params", self._h, _lib.ptr(out), _lib.stream_ptr(stream))
+        return out
+
+    def grads(self, stream=None):
+        torch = _torch()
+        out = torch.empty(self.n_params, dtype=torch.float32, device=self.device)
+        _lib.call("bd_unet_get_grads", self._h, _lib.ptr(out), _lib.stream_ptr(stream))
+        return out
+
+    def forward(self, a_noisy, props, flags=None, scale: float = 1e4, out=None, stream=None):
+        """Denoised absorbed map (same units and layout as a_noisy: fp32, nx*ny*nz, z fastest)."""
+        torch = _torch()
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        _lib.call("bd_unet_forward", self._h, _lib.ptr(a_noisy), _lib.ptr(props), _lib.ptr(flags), float(scale),
+                  _lib.ptr(out), _lib.stream_ptr(stream))
+        return out
+
+    def forward_backward(self, a_noisy, props, flags, target, scale: float = 1e4, loss_norm=None, pred=None,
+                         stream=None):
+        torch = _torch()
+        if pred is None:
+            pred = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        norm = loss_norm if loss_norm is not None else 1.0 / float(np.prod(self.shape))
+        _lib.call("bd_unet_forward_backward", self._h, _lib.ptr(a_noisy), _lib.ptr(props), _lib.ptr(flags),
+                  _lib.ptr(target), float(scale), float(norm), _lib.ptr(pred), _lib.stream_ptr(stream))
+        return pred
+
+    def adam(self, lr: float, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8, stream=None):
+        _lib.call("bd_unet_adam", self._h, float(lr), float(beta1), float(beta2), float(eps), _lib.stream_ptr(stream))
+
+    def read_loss(self, stream=None) -> float:
+        v = ctypes.c_double(0.0)
+        _lib.call("bd_unet_read_loss", self._h, ctypes.byref(v), _lib.stream_ptr(stream))
+        return float(v.value)
+
+
+def init_params(seed: int = 0):
+    """He-normal convolution weights, zero biases and a zero head: the untrained residual network
+    returns the noisy map unchanged (numpy float32 vector)."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for t, ci, co in LAYERS:
+        fan_in = t * ci if t == 27 else 9 * 12
+        w = rng.normal(0.0, np.sqrt(2.0 / fan_in), size=(t, co, ci))
+        if t == 9:
+            w[:, :, 12:] = 0.0      # the first layer's input channels 12-15 are always zero
+        parts += [w.ravel(), np.zeros(co)]
+    parts += [np.zeros(HEAD), np.zeros(1)]
+    return np.concatenate(parts).astype(np.float32)
