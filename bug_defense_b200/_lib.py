@@ -198,6 +198,7 @@ _SIGNATURES = {
     "bd_engine_set_mc": (c_int, [c_void_p, POINTER(McParams)]),
     "bd_engine_timing": (c_int, [c_void_p, c_int]),
     "bd_engine_timing_read": (c_int, [c_void_p, POINTER(c_double), POINTER(c_int64)]),
+    "bd_conv_plane_rows": (c_int64, [c_int, c_int, c_int]),
     "bd_conv_image_bytes": (c_int64, [c_int, c_int, c_int]),
     "bd_conv_pack_weights": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
     "bd_conv3d": (c_int, [POINTER(ConvCall), c_void_p]),

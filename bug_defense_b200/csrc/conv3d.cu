@@ -1,21 +1,29 @@
 // 3-D convolutions of the absorbed-map denoiser on the fifth-generation tensor cores.
 //
-// Volumes are channels-last bf16 rows with a one-voxel zero pad, so the neighbour (dx, dy, dz) of
-// row v is row v + dx*nyp*nzp + dy*nzp + dz for every interior voxel: a 3x3x3 convolution is 27
-// row-shifted GEMMs [128 voxels x cin] x [cin x cout] accumulated in TMEM (implicit GEMM).
+// Volumes are bf16 with a one-voxel zero pad, stored as "8-channel planes": channel c of padded row
+// v lives at ((c/8)*R + v)*8 + c%8, with R = padded rows + a zero margin. The neighbour (dx, dy, dz)
+// of row v is row v + dx*nyp*nzp + dy*nzp + dz for every interior voxel, so a 3x3x3 convolution is
+// 27 row-shifted GEMMs [128 voxels x cin] x [cin x cout] accumulated in TMEM (implicit GEMM), and
+// every operand tile is a run of contiguous 16-byte rows: one bulk copy per 8 channels.
 //
-// Forward / data-gradient kernel (k_conv): one CTA per SM walks 128-voxel tiles. For each of the
-// 9 (dx, dy) pairs a TMA load brings 130 consecutive rows (the tile plus one row either side) into
-// shared memory as cin/8 "planes" of 16-byte rows (the K-major, no-swizzle UMMA layout); the
-// three z taps are the same planes with the descriptor start moved by 0/16/32 bytes. Weights of
-// all taps stay resident in shared memory (one bulk copy per CTA). Warp 0 issues TMA, warp 1 owns
-// TMEM and issues tcgen05.mma, warps 2-5 drain double-buffered accumulators and run the fused
-// epilogue (bias, ReLU, nearest upsampling with the skip add, gradient gating, the 1x1 head).
+// Forward / data-gradient kernel (k_conv): persistent CTAs walk tiles of 128 consecutive rows. For
+// each of the 9 (dx, dy) pairs, cin/8 bulk copies bring the tile's rows shifted by (dx, dy) into
+// shared memory, which is exactly the K-major, no-swizzle UMMA layout. The three z taps are stacked
+// along N: one 128 x (3*cout) x 16 MMA per K step accumulates D[u][(dz, co)], and the epilogue
+// forms out[v] = D[v-1][dz=-1] + D[v][dz=0] + D[v+1][dz=+1] with warp shuffles (shared memory
+// across warp edges), so a tile yields 126 outputs (rows 1..126). A pipeline stage holds 9, 3 or 1
+// of a tile's runs (as shared memory allows), so the single MMA-issuing thread waits on one barrier
+// per stage, not per run; few, wide MMAs keep the tensor pipe's issue rate off the critical path
+// for the 16-channel layers. Weights of all taps stay resident in shared memory. Warp 0 issues the
+// copies, warp 1 owns TMEM and issues tcgen05.mma, warps 2-9 (two groups, one per accumulator)
+// drain the double-buffered accumulators and run the fused epilogue (bias, ReLU, nearest
+// upsampling with the skip add, gradient gating, the 1x1 head).
 //
 // Weight-gradient kernel (k_conv_wgrad): dW[t][co][ci] = sum_v g[v - off_t][co] x[v][ci]. Taps are
-// stacked along M (128/cout taps per MMA), with the shifted gradient tiles as an MN-major swizzled
-// A operand and the activation tile as MN-major B; each CTA reduces a contiguous range of 64-voxel
-// chunks in TMEM and adds its partial weights with FP32 atomics.
+// stacked along M (128/cout taps per MMA): 64-row plane chunks of the shifted gradient are the
+// MN-major, no-swizzle A operand (8 channels per 1 KB core-matrix column) and the activation chunks
+// are MN-major B; each CTA reduces a contiguous range of 64-voxel chunks in TMEM and adds its
+// partial weights with FP32 atomics.
 //
 // Every mbarrier wait is bounded; a timeout sets the error flag, the roles drain what they issued
 // and the CTA frees its TMEM and returns.
@@ -34,14 +42,18 @@ namespace bd {
 namespace {
 
 constexpr int kTileM = 128;
-constexpr int kPlaneBytes = 2176;      // 130 rows x 16 B, rounded up to a multiple of 128 B
+constexpr int kPlaneBytes = kTileM * 16;   // one 8-channel plane of a tile: 128 rows x 16 B
 constexpr int kSmemLimit = 232448;     // 227 KB opt-in dynamic shared memory per CTA
 constexpr int kWgradKv = 64;           // voxels per weight-gradient K chunk
+constexpr int kRowMargin = 256;        // zero rows after the padded volume (tile copies overrun it)
+constexpr int kEpiGroups = 2;          // epilogue warp groups (4 warps each), one per accumulator
+constexpr int kConvThreads = 64 + kEpiGroups * 128;
 
 struct Geom {
     int nxp, nyp, nzp;
     int v_lo, v_hi;       // interior rows lie in [v_lo, v_hi)
     int plane;            // nyp * nzp
+    int R;                // rows per 8-channel plane (padded rows + margin)
 };
 
 __host__ __device__ inline Geom make_geom(int nx, int ny, int nz) {
@@ -50,8 +62,11 @@ __host__ __device__ inline Geom make_geom(int nx, int ny, int nz) {
     g.plane = g.nyp * g.nzp;
     g.v_lo = g.plane + g.nzp + 1;
     g.v_hi = nx * g.plane + ny * g.nzp + nz + 1;
+    g.R = g.nxp * g.plane + kRowMargin;
     return g;
 }
+
+__device__ __forceinline__ size_t prow(const Geom& g, int chunk, int v) { return ((size_t)chunk * g.R + v) * 8; }
 
 __device__ __forceinline__ int tap_offset(const Geom& g, int t, int taps) {
     if (taps == 27) {
@@ -66,6 +81,7 @@ struct ConvArgs {
     Geom g;        // level of the convolution
     Geom gf;       // finer level (UPADD modes)
     int taps, mode, cout_total, n_off, n_tiles;
+    const __nv_bfloat16* input;
     const __nv_bfloat16* wimage;
     int wbytes;
     const float* bias;
@@ -90,36 +106,37 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
     return *reinterpret_cast<uint32_t*>(&h);
 }
 
+// N channels of row v, starting at 8-channel plane c0, from / to plane-layout storage.
 template <int N>
-__device__ __forceinline__ void store_row(__nv_bfloat16* dst, const float* v) {
+__device__ __forceinline__ void store_row(__nv_bfloat16* base, const Geom& g, int c0, int v, const float* val) {
 #pragma unroll
     for (int c = 0; c < N; c += 8) {
         uint4 q;
-        q.x = pack_bf16x2(v[c + 0], v[c + 1]);
-        q.y = pack_bf16x2(v[c + 2], v[c + 3]);
-        q.z = pack_bf16x2(v[c + 4], v[c + 5]);
-        q.w = pack_bf16x2(v[c + 6], v[c + 7]);
-        *reinterpret_cast<uint4*>(dst + c) = q;
+        q.x = pack_bf16x2(val[c + 0], val[c + 1]);
+        q.y = pack_bf16x2(val[c + 2], val[c + 3]);
+        q.z = pack_bf16x2(val[c + 4], val[c + 5]);
+        q.w = pack_bf16x2(val[c + 6], val[c + 7]);
+        *reinterpret_cast<uint4*>(base + prow(g, c0 + c / 8, v)) = q;
     }
 }
 
 template <int N>
-__device__ __forceinline__ void load_row(const __nv_bfloat16* src, float* v) {
+__device__ __forceinline__ void load_row(const __nv_bfloat16* base, const Geom& g, int c0, int v, float* val) {
 #pragma unroll
     for (int c = 0; c < N; c += 8) {
-        const uint4 q = *reinterpret_cast<const uint4*>(src + c);
+        const uint4 q = *reinterpret_cast<const uint4*>(base + prow(g, c0 + c / 8, v));
         const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&q);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const float2 f = __bfloat1622float2(h[j]);
-            v[c + 2 * j] = f.x;
-            v[c + 2 * j + 1] = f.y;
+            val[c + 2 * j] = f.x;
+            val[c + 2 * j + 1] = f.y;
         }
     }
 }
 
 struct SharedCtl {
-    unsigned long long full[8], empty[8];
+    unsigned long long full[32], empty[32];
     unsigned long long wfull, acc_full[2], acc_empty[2], done;
     uint32_t tmem;
     volatile int abort;
@@ -132,16 +149,24 @@ __device__ __forceinline__ bool wait_or_abort(unsigned long long* bar, unsigned 
     return false;
 }
 
+constexpr int pow2_at_least(int x) { return x <= 32 ? 32 : x <= 64 ? 64 : x <= 128 ? 128 : x <= 256 ? 256 : 512; }
+
 template <int CIN, int N>
 struct ConvCfg {
     static constexpr int KP = CIN / 8;
-    static constexpr int STAGE = KP * kPlaneBytes;
+    static constexpr int RUN = KP * kPlaneBytes;   // one (dx, dy)-shifted run of a tile
     static constexpr int WMAX = 27 * CIN * N * 2;
-    static constexpr int CTL = 1024;  // SharedCtl, padded
-    static constexpr int NST_FIT = (kSmemLimit - 1024 - CTL - WMAX) / STAGE;
-    static constexpr int NST = NST_FIT > 8 ? 8 : NST_FIT;
+    static constexpr int XB = 2 * 2 * 2 * 4 * N;  // floats: edge exchange [group][parity][side][quad][N]
+    static constexpr int CTL = 1024 + ((XB * 4 + 256 + 1023) / 1024) * 1024;  // SharedCtl + exchange + bias
+    static constexpr int AVAIL = kSmemLimit - 1024 - CTL - WMAX;
+    // runs per pipeline stage: as many of the 9 as keep >= 3 stages, so the single MMA-issuing
+    // thread waits on few barriers per tile
+    static constexpr int RPS = AVAIL / (9 * RUN) >= 3 ? 9 : AVAIL / (3 * RUN) >= 3 ? 3 : 1;
+    static constexpr int STAGE = RPS * RUN;
+    static constexpr int NST_FIT = AVAIL / STAGE;
+    static constexpr int NST = NST_FIT > 32 ? 32 : NST_FIT;
     static constexpr int SMEM = 1024 + CTL + WMAX + NST * STAGE;
-    static constexpr int TMEM_COLS = (2 * N) < 32 ? 32 : 2 * N;
+    static constexpr int TMEM_COLS = pow2_at_least(2 * 3 * N);   // two accumulators of 3N columns
     static_assert(NST >= 3, "conv: not enough shared memory for a 3-stage pipeline");
     static_assert(SMEM <= kSmemLimit, "conv: shared memory over the limit");
 };
@@ -153,50 +178,46 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs& a, int v, float* a
     const int x = v / g.plane, r = v - x * g.plane, y = r / g.nzp, z = r - y * g.nzp;
     if (v >= g.v_hi || y < 1 || y > g.nyp - 2 || z < 1 || z > g.nzp - 2) return;
     const int mode = a.mode;
-    if (mode <= BD_CONV_FWD_HEAD && a.bias) {
-#pragma unroll
-        for (int c = 0; c < N; ++c) acc[c] += a.bias[c];
-    }
     if (mode <= BD_CONV_FWD_HEAD) {
 #pragma unroll
         for (int c = 0; c < N; ++c) acc[c] = fmaxf(acc[c], 0.f);
     }
+    const int c0 = a.n_off / 8;
     if (mode == BD_CONV_FWD_RELU || mode == BD_CONV_BWD_RAW) {
-        store_row<N>(a.out + (size_t)v * a.cout_total + a.n_off, acc);
+        store_row<N>(a.out, g, c0, v, acc);
     } else if (mode == BD_CONV_BWD_MASK) {
-        const __nv_bfloat16* am = a.aux + (size_t)v * a.cout_total + a.n_off;
 #pragma unroll
         for (int c = 0; c < N; c += 8) {
             float m[8];
-            load_row<8>(am + c, m);
+            load_row<8>(a.aux, g, c0 + c / 8, v, m);
 #pragma unroll
             for (int j = 0; j < 8; ++j) acc[c + j] = m[j] > 0.f ? acc[c + j] : 0.f;
         }
-        store_row<N>(a.out + (size_t)v * a.cout_total + a.n_off, acc);
+        store_row<N>(a.out, g, c0, v, acc);
     } else if (mode == BD_CONV_FWD_UPADD || mode == BD_CONV_BWD_UPADD) {
-        if (mode == BD_CONV_FWD_UPADD && a.out_coarse)
-            store_row<N>(a.out_coarse + (size_t)v * a.cout_total + a.n_off, acc);
+        if (mode == BD_CONV_FWD_UPADD && a.out_coarse) store_row<N>(a.out_coarse, g, c0, v, acc);
         const Geom& f = a.gf;
         for (int ch = 0; ch < 8; ++ch) {
             const int fx = 2 * x - 1 + (ch >> 2), fy = 2 * y - 1 + ((ch >> 1) & 1), fz = 2 * z - 1 + (ch & 1);
-            const size_t vf = ((size_t)fx * f.plane + (size_t)fy * f.nzp + fz) * a.cout_total + a.n_off;
+            const int vf = fx * f.plane + fy * f.nzp + fz;
 #pragma unroll
             for (int c = 0; c < N; c += 8) {
                 float s[8], o[8];
-                load_row<8>(a.aux + vf + c, s);
+                load_row<8>(a.aux, f, c0 + c / 8, vf, s);
                 if (mode == BD_CONV_FWD_UPADD) {
 #pragma unroll
                     for (int j = 0; j < 8; ++j) o[j] = acc[c + j] + s[j];
                 } else {
                     float m[8];
-                    load_row<8>(a.aux2 + vf + c, m);
+                    load_row<8>(a.aux2, f, c0 + c / 8, vf, m);
 #pragma unroll
                     for (int j = 0; j < 8; ++j) o[j] = m[j] > 0.f ? s[j] + 0.125f * acc[c + j] : 0.f;
                 }
-                store_row<8>(a.out + vf + c, o);
+                store_row<8>(a.out, f, c0 + c / 8, vf, o);
             }
         }
-    } else if (mode == BD_CONV_FWD_HEAD) {
+    } else if constexpr (N == 16) {
+        if (mode != BD_CONV_FWD_HEAD) return;
         const int nz = g.nzp - 2, ny = g.nyp - 2;
         const size_t u = ((size_t)(x - 1) * ny + (y - 1)) * nz + (z - 1);
         float yv = a.head[N];
@@ -216,13 +237,13 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs& a, int v, float* a
                 head_acc[c] = fmaf(dy, acc[c], head_acc[c]);
             }
             head_acc[N] += dy;
-            store_row<N>(a.grad_out + (size_t)v * N, gr);
+            store_row<N>(a.grad_out, g, 0, v, gr);
         }
     }
 }
 
 template <int CIN, int N>
-__global__ void __launch_bounds__(192, 1) k_conv(const __grid_constant__ CUtensorMap tin, const ConvArgs a) {
+__global__ void __launch_bounds__(kConvThreads, 1) k_conv(const ConvArgs a) {
     using C = ConvCfg<CIN, N>;
     extern __shared__ unsigned char smem_raw[];
     const uint32_t base_addr = smem_addr(smem_raw);
@@ -231,9 +252,13 @@ __global__ void __launch_bounds__(192, 1) k_conv(const __grid_constant__ CUtenso
     unsigned char* wsm = smem + C::CTL;
     unsigned char* stages = wsm + C::WMAX;
 
+    float* xbuf = reinterpret_cast<float*>(smem + 1024);
+    float* sbias = xbuf + C::XB;                    // [N] bias of the slice (forward modes), else 0
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int kz = a.taps == 27 ? 3 : 1;
-    const int rows = kz == 3 ? kTileM + 2 : kTileM;
+    const int NN = kz * N;                          // MMA N: z taps stacked along N
+    const int out_per_tile = kz == 3 ? kTileM - 2 : kTileM;
+    const int u_base = a.g.v_lo - (kz == 3 ? 1 : 0);
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < C::NST; ++s) {
@@ -249,6 +274,8 @@ __global__ void __launch_bounds__(192, 1) k_conv(const __grid_constant__ CUtenso
         ctl->abort = 0;
         mbar_init_fence();
     }
+    for (int c = threadIdx.x; c < N; c += blockDim.x)
+        sbias[c] = (a.mode <= BD_CONV_FWD_HEAD && a.bias) ? a.bias[c] : 0.f;
     if (warp == 1) tmem_alloc(&ctl->tmem, C::TMEM_COLS);
     tc_fence_before();
     __syncthreads();
@@ -257,7 +284,7 @@ __global__ void __launch_bounds__(192, 1) k_conv(const __grid_constant__ CUtenso
 
     if (warp == 0) {
         if (lane == 0) {
-            // ---- producer: resident weights, then 9 (dx, dy) row tiles per 128-voxel tile ----
+            // ---- producer: resident weights, then 9 (dx, dy)-shifted row runs per tile ----
             mbar_expect_tx(&ctl->wfull, a.wbytes);
             for (int off = 0; off < a.wbytes; off += 32768)
                 bulk_load(wsm + off, reinterpret_cast<const unsigned char*>(a.wimage) + off,
@@ -266,15 +293,20 @@ __global__ void __launch_bounds__(192, 1) k_conv(const __grid_constant__ CUtenso
             unsigned ph = 0;
             long long issued = 0;
             for (int tile = blockIdx.x; tile < a.n_tiles && !ctl->abort; tile += gridDim.x) {
-                const int v0 = a.g.v_lo + tile * kTileM;
-                for (int q = 0; q < 9; ++q) {
+                const int u0 = u_base + tile * out_per_tile;
+                for (int q0 = 0; q0 < 9; q0 += C::RPS) {
                     if (!wait_or_abort(&ctl->empty[s], ph ^ 1, ctl, a.err)) break;
-                    const int dx = q / 3 - 1, dy = q % 3 - 1;
-                    const int row0 = v0 + dx * a.g.plane + dy * a.g.nzp - (kz == 3 ? 1 : 0);
                     unsigned char* st = stages + s * C::STAGE;
-                    mbar_expect_tx(&ctl->full[s], C::KP * rows * 16);
+                    mbar_expect_tx(&ctl->full[s], C::STAGE);
 #pragma unroll
-                    for (int p = 0; p < C::KP; ++p) tma_load_2d(st + p * kPlaneBytes, &tin, 8 * p, row0, &ctl->full[s]);
+                    for (int r = 0; r < C::RPS; ++r) {
+                        const int q = q0 + r;
+                        const int row0 = u0 + (q / 3 - 1) * a.g.plane + (q % 3 - 1) * a.g.nzp;
+#pragma unroll
+                        for (int p = 0; p < C::KP; ++p)
+                            bulk_load(st + r * C::RUN + p * kPlaneBytes, a.input + prow(a.g, p, row0), kPlaneBytes,
+                                      &ctl->full[s]);
+                    }
                     ++issued;
                     if (++s == C::NST) { s = 0; ph ^= 1; }
                 }
@@ -289,28 +321,30 @@ __global__ void __launch_bounds__(192, 1) k_conv(const __grid_constant__ CUtenso
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            // ---- MMA issuer ----
-            const uint32_t idesc = umma_idesc_bf16(kTileM, N, false, false);
+            // ---- MMA issuer: per (dx, dy) stage, CIN/16 MMAs of 128 x NN x 16 ----
+            const uint32_t idesc = umma_idesc_bf16(kTileM, NN, false, false);
             const uint32_t wbase = smem_addr(wsm), sbase = smem_addr(stages);
+            const uint32_t wq = C::KP * NN * 16;    // weight image bytes per (dx, dy) pair
             bool ok = wait_or_abort(&ctl->wfull, 0, ctl, a.err);
             int s = 0, acc = 0;
             unsigned ph = 0, aph = 0;
             for (int tile = blockIdx.x; ok && tile < a.n_tiles && !ctl->abort; tile += gridDim.x) {
                 if (!wait_or_abort(&ctl->acc_empty[acc], aph ^ 1, ctl, a.err)) break;
                 tc_fence_after();
-                const uint32_t d = tmem + acc * N;
-                for (int q = 0; q < 9 && ok; ++q) {
+                const uint32_t d = tmem + acc * NN;
+                for (int q0 = 0; q0 < 9 && ok; q0 += C::RPS) {
                     if (!wait_or_abort(&ctl->full[s], ph, ctl, a.err)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t st = sbase + s * C::STAGE;
-                    for (int dz = 0; dz < kz; ++dz) {
-                        const int t = q * kz + dz;
+#pragma unroll
+                    for (int r = 0; r < C::RPS; ++r) {
+                        const int q = q0 + r;
 #pragma unroll
                         for (int kk = 0; kk < CIN / 16; ++kk) {
-                            const uint64_t ad = umma_desc(st + dz * 16 + kk * 2 * kPlaneBytes, kPlaneBytes, 128, UMMA_NONE);
-                            const uint64_t bd = umma_desc(wbase + t * (C::KP * N * 16) + kk * 2 * (N * 16), N * 16, 128,
+                            const uint64_t ad = umma_desc(st + r * C::RUN + kk * 2 * kPlaneBytes, kPlaneBytes, 128,
                                                           UMMA_NONE);
-                            umma_bf16(d, ad, bd, idesc, (q | dz | kk) != 0);
+                            const uint64_t bd = umma_desc(wbase + q * wq + kk * 2 * (NN * 16), NN * 16, 128, UMMA_NONE);
+                            umma_bf16(d, ad, bd, idesc, (q | kk) != 0);
                         }
                     }
                     umma_commit(&ctl->empty[s]);
@@ -325,34 +359,87 @@ __global__ void __launch_bounds__(192, 1) k_conv(const __grid_constant__ CUtenso
             mbar_wait(&ctl->done, 0);
         }
     } else {
-        // ---- epilogue warps 2..5: TMEM lanes 32*(warp % 4) .. +31 ----
+        // ---- epilogue: two groups of 4 warps (2..5, 6..9); group g drains accumulator g, i.e.
+        // every other tile of this CTA. Warp w reads TMEM lanes 32*(w % 4) .. +31; row = TMEM lane.
+        const int grp = (warp - 2) >> 2;
         const int quad = warp & 3;
         const int row = quad * 32 + lane;
-        int acc = 0;
+        const int acc = grp;
         unsigned aph = 0;
-        float head_acc[17];
+        constexpr int HA = N == 16 ? 17 : 1;        // head gradient accumulators (16-channel head only)
+        float head_acc[HA];
 #pragma unroll
-        for (int c = 0; c < 17; ++c) head_acc[c] = 0.f;
+        for (int c = 0; c < HA; ++c) head_acc[c] = 0.f;
         double loss_acc = 0.0;
-        for (int tile = blockIdx.x; tile < a.n_tiles; tile += gridDim.x) {
-            if (!wait_or_abort(&ctl->acc_full[acc], aph, ctl, a.err)) break;
-            tc_fence_after();
+        int par = 0;
+        for (int tile = blockIdx.x + grp * gridDim.x; tile < a.n_tiles; tile += kEpiGroups * gridDim.x) {
+            // a timed-out wait still takes part in the group's named barrier below, so its four
+            // warps stay in step; the tile is then skipped
+            const bool okw = !ctl->abort && wait_or_abort(&ctl->acc_full[acc], aph, ctl, a.err);
             float v[N];
+            float* xb0 = xbuf + (((grp * 2 + par) * 2 + 0) * 4) * N;   // lane 31's dz=-1 block, per quad
+            float* xb2 = xbuf + (((grp * 2 + par) * 2 + 1) * 4) * N;   // lane 0's dz=+1 block, per quad
+            if (okw) {
+                tc_fence_after();
+                const uint32_t tb = tmem + ((uint32_t)(quad * 32) << 16) + acc * NN;
+                if (kz == 3) {
 #pragma unroll
-            for (int c = 0; c < N; c += 16) tmem_ld16(tmem + ((uint32_t)(quad * 32) << 16) + acc * N + c, v + c);
-            tmem_ld_wait();
-            tc_fence_before();
+                    for (int c = 0; c < N; c += 16) {
+                        float t0[16], t1[16], t2[16];
+                        tmem_ld16(tb + c, t0);
+                        tmem_ld16(tb + N + c, t1);
+                        tmem_ld16(tb + 2 * N + c, t2);
+                        tmem_ld_wait();
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            const float up = __shfl_up_sync(0xffffffffu, t0[j], 1);
+                            const float dn = __shfl_down_sync(0xffffffffu, t2[j], 1);
+                            v[c + j] = t1[j] + (lane > 0 ? up : 0.f) + (lane < 31 ? dn : 0.f);
+                        }
+                        if (lane == 31) {
+#pragma unroll
+                            for (int j = 0; j < 16; ++j) xb0[quad * N + c + j] = t0[j];
+                        }
+                        if (lane == 0) {
+#pragma unroll
+                            for (int j = 0; j < 16; ++j) xb2[quad * N + c + j] = t2[j];
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < N; c += 16) tmem_ld16(tb + c, v + c);
+                    tmem_ld_wait();
+                }
+                tc_fence_before();
+            }
             mbar_arrive(&ctl->acc_empty[acc]);
-            acc ^= 1;
-            if (acc == 0) aph ^= 1;
-            conv_epilogue<N>(a, a.g.v_lo + tile * kTileM + row, v, head_acc, loss_acc);
+            asm volatile("bar.sync %0, 128;" ::"r"(1 + grp) : "memory");
+            if (okw && kz == 3) {
+                if (lane == 0 && quad > 0) {
+#pragma unroll
+                    for (int c = 0; c < N; ++c) v[c] += xb0[(quad - 1) * N + c];
+                }
+                if (lane == 31 && quad < 3) {
+#pragma unroll
+                    for (int c = 0; c < N; ++c) v[c] += xb2[(quad + 1) * N + c];
+                }
+            }
+            const int u0 = u_base + tile * out_per_tile;
+            const bool out_row = kz == 1 || (row >= 1 && row <= kTileM - 2);
+            if (okw && out_row && !ctl->abort) {
+#pragma unroll
+                for (int c = 0; c < N; ++c) v[c] += sbias[c];
+                conv_epilogue<N>(a, u0 + row, v, head_acc, loss_acc);
+            }
+            aph ^= 1;
+            par ^= 1;
         }
         if (a.mode == BD_CONV_FWD_HEAD && a.target) {
 #pragma unroll
-            for (int c = 0; c < 17; ++c) {
+            for (int c = 0; c < HA; ++c) {
                 float h = head_acc[c];
                 for (int o = 16; o; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
-                if (lane == 0 && c <= N) atomicAdd(&a.head_grad[c], h);
+                if (lane == 0) atomicAdd(&a.head_grad[c], h);
             }
             for (int o = 16; o; o >>= 1) loss_acc += __shfl_xor_sync(0xffffffffu, loss_acc, o);
             if (lane == 0) atomicAdd(a.loss, loss_acc);
@@ -371,6 +458,8 @@ __global__ void __launch_bounds__(192, 1) k_conv(const __grid_constant__ CUtenso
 struct WgradArgs {
     Geom g;
     int taps, g0, g1, chunks_total, chunks_per_cta;
+    const __nv_bfloat16* grad;
+    const __nv_bfloat16* act;
     float* dw;
     int* err;
 };
@@ -378,11 +467,13 @@ struct WgradArgs {
 template <int COUT, int CIN>
 struct WgradCfg {
     static constexpr int TPG = kTileM / COUT;               // taps per group (stacked along M)
-    static constexpr int ABOX = kWgradKv * COUT * 2;        // one tap's gradient tile
-    static constexpr int BBOX = kWgradKv * CIN * 2;         // activation tile
+    static constexpr int CHUNK = kWgradKv * 16;             // 64 rows of one 8-channel plane (1 KB)
+    static constexpr int ABOX = (COUT / 8) * CHUNK;         // one tap's gradient tile
+    static constexpr int BBOX = (CIN / 8) * CHUNK;          // activation tile
     static constexpr int STAGE = TPG * ABOX + BBOX;
-    static constexpr int NST = 6;
     static constexpr int CTL = 1024;
+    static constexpr int NST_FIT = (kSmemLimit - 1024 - CTL) / STAGE;
+    static constexpr int NST = NST_FIT > 12 ? 12 : NST_FIT;
     static constexpr int SMEM = 1024 + CTL + NST * STAGE;
     static constexpr int GMAX = (512 / CIN) < 14 ? (512 / CIN) : 14;   // groups per launch (TMEM columns)
     static_assert(SMEM <= kSmemLimit, "wgrad: shared memory over the limit");
@@ -390,8 +481,7 @@ struct WgradCfg {
 };
 
 template <int COUT, int CIN>
-__global__ void __launch_bounds__(192, 1) k_conv_wgrad(const __grid_constant__ CUtensorMap tg,
-                                                       const __grid_constant__ CUtensorMap tx, const WgradArgs a) {
+__global__ void __launch_bounds__(192, 1) k_conv_wgrad(const WgradArgs a) {
     using C = WgradCfg<COUT, CIN>;
     extern __shared__ unsigned char smem_raw[];
     const uint32_t base_addr = smem_addr(smem_raw);
@@ -436,9 +526,16 @@ __global__ void __launch_bounds__(192, 1) k_conv_wgrad(const __grid_constant__ C
 #pragma unroll
                     for (int j = 0; j < C::TPG; ++j) {
                         const int t = min(gi * C::TPG + j, a.taps - 1);
-                        tma_load_2d(st + j * C::ABOX, &tg, 0, v0 - tap_offset(a.g, t, a.taps), &ctl->full[s]);
+                        const int row = v0 - tap_offset(a.g, t, a.taps);
+#pragma unroll
+                        for (int cb = 0; cb < COUT / 8; ++cb)
+                            bulk_load(st + j * C::ABOX + cb * C::CHUNK, a.grad + prow(a.g, cb, row), C::CHUNK,
+                                      &ctl->full[s]);
                     }
-                    tma_load_2d(st + C::TPG * C::ABOX, &tx, 0, v0, &ctl->full[s]);
+#pragma unroll
+                    for (int cb = 0; cb < CIN / 8; ++cb)
+                        bulk_load(st + C::TPG * C::ABOX + cb * C::CHUNK, a.act + prow(a.g, cb, v0), C::CHUNK,
+                                  &ctl->full[s]);
                     ++issued;
                     if (++s == C::NST) { s = 0; ph ^= 1; }
                 }
@@ -451,10 +548,10 @@ __global__ void __launch_bounds__(192, 1) k_conv_wgrad(const __grid_constant__ C
         }
     } else if (warp == 1) {
         if (lane == 0) {
+            // MN-major, no swizzle: 8 M (or N) elements x 8 K rows per 128-byte core matrix; K groups
+            // 128 B apart (LBO), 8-element M/N blocks one 1 KB chunk apart (SBO)
             const uint32_t idesc = umma_idesc_bf16(kTileM, CIN, true, true);
             const uint32_t sbase = smem_addr(stages);
-            constexpr uint32_t sbo_a = 8 * COUT * 2, sbo_b = 8 * CIN * 2;
-            constexpr uint32_t lay_a = umma_swizzle_for_bytes(COUT * 2), lay_b = umma_swizzle_for_bytes(CIN * 2);
             int s = 0;
             unsigned ph = 0;
             bool ok = true;
@@ -466,8 +563,8 @@ __global__ void __launch_bounds__(192, 1) k_conv_wgrad(const __grid_constant__ C
                     const uint32_t d = tmem + (gi - a.g0) * CIN;
 #pragma unroll
                     for (int kk = 0; kk < kWgradKv / 16; ++kk) {
-                        const uint64_t ad = umma_desc(st + kk * 2 * sbo_a, C::ABOX, sbo_a, lay_a);
-                        const uint64_t bd = umma_desc(st + C::TPG * C::ABOX + kk * 2 * sbo_b, C::BBOX, sbo_b, lay_b);
+                        const uint64_t ad = umma_desc(st + kk * 256, 128, C::CHUNK, UMMA_NONE);
+                        const uint64_t bd = umma_desc(st + C::TPG * C::ABOX + kk * 256, 128, C::CHUNK, UMMA_NONE);
                         umma_bf16(d, ad, bd, idesc, (c != c_begin) || kk != 0);
                     }
                     umma_commit(&ctl->empty[s]);
@@ -508,16 +605,21 @@ __global__ void __launch_bounds__(192, 1) k_conv_wgrad(const __grid_constant__ C
 
 __global__ void k_pack_weights(int taps, int cin, int cout, int n_off, int n_slice, int transpose, const float* w,
                                __nv_bfloat16* img) {
-    // image[t][kp][n][8]: K-major planes of 8 input channels for each of the n_slice outputs
+    // image[q][kp][dz][n][8]: for each (dx, dy) pair q, K-major planes of 8 input channels whose
+    // rows are the (z tap, output) pairs the stacked MMA computes (kz = 3 z taps, or 1)
     const int K = transpose ? cout : cin;
+    const int kz = taps == 27 ? 3 : 1;
     const long long total = (long long)taps * K * n_slice;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
         const int j = (int)(i & 7);
         long long r = i >> 3;
         const int n = (int)(r % n_slice);
         r /= n_slice;
+        const int dz = (int)(r % kz);
+        r /= kz;
         const int kp = (int)(r % (K / 8));
-        const int t = (int)(r / (K / 8));
+        const int q = (int)(r / (K / 8));
+        const int t = q * kz + dz;
         const int k = kp * 8 + j;
         float val;
         if (!transpose) val = w[((size_t)t * cout + (n_off + n)) * cin + k];
@@ -530,15 +632,13 @@ template <int CIN, int N>
 int launch_conv_t(const BdConvCall& c, cudaStream_t st, int* err, int sms) {
     using C = ConvCfg<CIN, N>;
     const Geom g = make_geom(c.nx, c.ny, c.nz);
-    CUtensorMap tin;
-    const int rows = c.taps == 27 ? kTileM + 2 : kTileM;
-    if (!make_tmap_2d_bf16(&tin, c.input, (long long)g.nxp * g.plane, CIN, 8, rows, 0))
-        return fail(BD_ERR_INVALID_ARG, "bd_conv3d: tensor map for the input could not be encoded");
     ConvArgs a{};
     a.g = g;
     a.gf = make_geom(2 * c.nx, 2 * c.ny, 2 * c.nz);
     a.taps = c.taps; a.mode = c.mode; a.cout_total = c.cout_total; a.n_off = c.n_off;
-    a.n_tiles = (g.v_hi - g.v_lo + kTileM - 1) / kTileM;
+    const int per_tile = c.taps == 27 ? kTileM - 2 : kTileM;
+    a.n_tiles = (g.v_hi - g.v_lo + per_tile - 1) / per_tile;
+    a.input = static_cast<const __nv_bfloat16*>(c.input);
     a.wimage = static_cast<const __nv_bfloat16*>(c.wimage);
     a.wbytes = (int)bd_conv_image_bytes(c.taps, CIN, N);
     a.bias = c.bias;
@@ -551,8 +651,10 @@ int launch_conv_t(const BdConvCall& c, cudaStream_t st, int* err, int sms) {
     a.grad_out = static_cast<__nv_bfloat16*>(c.grad_out);
     a.err = err;
     BD_CUDA(cudaFuncSetAttribute(k_conv<CIN, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
-    const int grid = std::max(1, std::min(a.n_tiles, sms));
-    k_conv<CIN, N><<<grid, 192, C::SMEM, st>>>(tin, a);
+    int occ = 1;
+    BD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv<CIN, N>, kConvThreads, C::SMEM));
+    const int grid = std::max(1, std::min(a.n_tiles, sms * std::max(1, occ)));
+    k_conv<CIN, N><<<grid, kConvThreads, C::SMEM, st>>>(a);
     BD_CHECK_LAUNCH("k_conv");
     return BD_OK;
 }
@@ -561,17 +663,13 @@ template <int COUT, int CIN>
 int launch_wgrad_t(int nx, int ny, int nz, int taps, const void* grad, const void* act, float* dw, cudaStream_t st,
                    int* err, int sms) {
     using C = WgradCfg<COUT, CIN>;
-    const Geom g = make_geom(nx, ny, nz);
-    const long long rows = (long long)g.nxp * g.plane;
-    CUtensorMap tg, tx;
-    if (!make_tmap_2d_bf16(&tg, grad, rows, COUT, COUT, kWgradKv, COUT * 2) ||
-        !make_tmap_2d_bf16(&tx, act, rows, CIN, CIN, kWgradKv, CIN * 2))
-        return fail(BD_ERR_INVALID_ARG, "bd_conv3d_wgrad: tensor maps could not be encoded");
     BD_CUDA(cudaFuncSetAttribute(k_conv_wgrad<COUT, CIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
     WgradArgs a{};
-    a.g = g;
+    a.g = make_geom(nx, ny, nz);
     a.taps = taps;
-    a.chunks_total = (g.v_hi - g.v_lo + kWgradKv - 1) / kWgradKv;
+    a.chunks_total = (a.g.v_hi - a.g.v_lo + kWgradKv - 1) / kWgradKv;
+    a.grad = static_cast<const __nv_bfloat16*>(grad);
+    a.act = static_cast<const __nv_bfloat16*>(act);
     a.dw = dw;
     a.err = err;
     const int groups = (taps + C::TPG - 1) / C::TPG;
@@ -582,7 +680,7 @@ int launch_wgrad_t(int nx, int ny, int nz, int taps, const void* grad, const voi
     for (int g0 = 0; g0 < groups; g0 += C::GMAX) {
         a.g0 = g0;
         a.g1 = std::min(groups, g0 + C::GMAX);
-        k_conv_wgrad<COUT, CIN><<<grid, 192, C::SMEM, st>>>(tg, tx, a);
+        k_conv_wgrad<COUT, CIN><<<grid, 192, C::SMEM, st>>>(a);
         BD_CHECK_LAUNCH("k_conv_wgrad");
     }
     return BD_OK;
@@ -618,6 +716,9 @@ int conv_check(const BdConvCall& c) {
         BD_REQUIRE(c.aux != nullptr && (c.mode == BD_CONV_FWD_UPADD || c.aux2 != nullptr),
                    "bd_conv3d: the upsampling modes need aux (and aux2)");
     if (c.mode == BD_CONV_BWD_MASK) BD_REQUIRE(c.aux != nullptr, "bd_conv3d: BWD_MASK needs aux");
+    BD_REQUIRE(((uintptr_t)c.input | (uintptr_t)c.wimage | (uintptr_t)c.out | (uintptr_t)c.aux | (uintptr_t)c.aux2 |
+                (uintptr_t)c.out_coarse | (uintptr_t)c.grad_out) % 16 == 0,
+               "bd_conv3d: volumes and weight images must be 16-byte aligned");
     if (c.mode == BD_CONV_FWD_HEAD) {
         BD_REQUIRE(c.n_slice == 16 && c.cout_total == 16 && c.n_off == 0, "bd_conv3d: the head takes 16 channels");
         BD_REQUIRE(c.head && c.a_noisy && c.mask && c.pred && c.scale > 0.f, "bd_conv3d: head inputs missing");
@@ -681,6 +782,10 @@ static int run_checked(cudaStream_t st, const char* what, F launch) {
 
 using namespace bd;
 
+extern "C" int64_t bd_conv_plane_rows(int nx, int ny, int nz) {
+    return (int64_t)(nx + 2) * (ny + 2) * (nz + 2) + kRowMargin;
+}
+
 extern "C" int64_t bd_conv_image_bytes(int taps, int k_channels, int n_slice) {
     return (int64_t)taps * k_channels * n_slice * 2;
 }
@@ -709,6 +814,7 @@ extern "C" int bd_conv3d_wgrad(int nx, int ny, int nz, int cin, int cout, int ta
                "bd_conv3d_wgrad: channels must be 16, 32 or 64");
     BD_REQUIRE(taps == 27 || taps == 9, "bd_conv3d_wgrad: taps must be 27 or 9");
     BD_REQUIRE((long long)(nx + 2) * (ny + 2) * (nz + 2) * 64 < (1LL << 31), "bd_conv3d_wgrad: volume too large");
+    BD_REQUIRE(((uintptr_t)grad | (uintptr_t)act) % 16 == 0, "bd_conv3d_wgrad: volumes must be 16-byte aligned");
     cudaStream_t st = (cudaStream_t)stream;
     return run_checked(st, "bd_conv3d_wgrad",
                        [&](int* err) { return wgrad_launch(nx, ny, nz, cin, cout, taps, grad, act, dw, st, err); });

@@ -1,8 +1,7 @@
-// Tensor-map encoding for the TMA-fed kernels (stencils and the denoiser's convolutions).
+// Tensor-map encoding for the TMA-fed stencil kernels.
 #include <cuda.h>
 
 #include "tma.cuh"
-#include "umma.cuh"
 
 namespace bd {
 
@@ -37,27 +36,6 @@ bool make_tmap_3d_f32(CUtensorMap* out, const void* base, int nx, int ny, int nz
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(base), dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS;
-}
-
-bool make_tmap_2d_bf16(CUtensorMap* out, const void* base, long long rows, int cols, int bc, int br, int swizzle) {
-    if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || (cols * 2) % 16 != 0 || (bc * 2) % 16 != 0) return false;
-    if (bc > 256 || br > 256 || bc > cols) return false;
-    CUtensorMapSwizzle sw = CU_TENSOR_MAP_SWIZZLE_NONE;
-    if (swizzle == 32) sw = CU_TENSOR_MAP_SWIZZLE_32B;
-    else if (swizzle == 64) sw = CU_TENSOR_MAP_SWIZZLE_64B;
-    else if (swizzle == 128) sw = CU_TENSOR_MAP_SWIZZLE_128B;
-    else if (swizzle != 0) return false;
-    if (swizzle != 0 && bc * 2 != swizzle) return false;
-    EncodeTiledFn fn = encode_tiled();
-    if (!fn) return false;
-    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-    cuuint32_t box[2] = {(cuuint32_t)bc, (cuuint32_t)br};
-    cuuint32_t estr[2] = {1, 1};
-    CUresult r = fn(out, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }

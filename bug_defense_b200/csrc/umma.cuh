@@ -10,9 +10,9 @@
 //                    [10,13) B format (1 = bf16), [15] A major (0 K, 1 MN), [16] B major,
 //                    [17,23) N >> 3, [24,29) M >> 4
 // Canonical layouts used here (element = bf16, "core matrix" = 8 rows x 16 bytes):
-//   K-major, no swizzle: rows of 16 B (8 K-elements), 8-row groups SBO apart, K chunks LBO apart.
-//   MN-major, swizzle S (32/64/128 B): S bytes of MN-contiguous elements per K-row, 8 K-rows per
-//   atom, atoms along K SBO apart, atoms along MN LBO apart.
+//   K-major, no swizzle:  rows of 16 B (8 K-elements), 8-row groups SBO apart, K chunks LBO apart.
+//   MN-major, no swizzle: K-rows of 16 B (8 MN-elements), 8 K-rows per 128-byte core matrix,
+//                         K groups LBO apart, 8-element MN blocks SBO apart.
 #pragma once
 
 #include <cstdint>
@@ -22,10 +22,6 @@
 namespace bd {
 
 enum UmmaLayout : uint32_t { UMMA_NONE = 0, UMMA_SW128 = 2, UMMA_SW64 = 4, UMMA_SW32 = 6 };
-
-__host__ __device__ constexpr uint32_t umma_swizzle_for_bytes(int row_bytes) {
-    return row_bytes == 128 ? UMMA_SW128 : row_bytes == 64 ? UMMA_SW64 : row_bytes == 32 ? UMMA_SW32 : UMMA_NONE;
-}
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo, uint32_t layout) {
     uint64_t d = 0;
@@ -100,22 +96,9 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
         : "memory");
 }
 
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int c0, int c1,
-                                            unsigned long long* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
-        "[%4];" ::"r"(smem_addr(dst)),
-        "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(smem_addr(bar))
-        : "memory");
-}
-
 // Plain arrive (count 1) on an mbarrier.
 __device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
-
-// 2-D tiled map over a row-major bf16 matrix [rows][cols] (cols innermost); box {bc, br}; swizzle
-// given in bytes (0 = none, 32, 64, 128). Out-of-range rows read as zero.
-bool make_tmap_2d_bf16(CUtensorMap* out, const void* base, long long rows, int cols, int bc, int br, int swizzle);
 
 }  // namespace bd

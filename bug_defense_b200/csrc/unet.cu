@@ -37,11 +37,17 @@ long long param_count() {
 
 struct Level {
     int nx, ny, nz;
-    long long rows() const { return (long long)(nx + 2) * (ny + 2) * (nz + 2); }
+    long long rows() const { return bd_conv_plane_rows(nx, ny, nz); }   // per 8-channel plane
 };
 
 __device__ __forceinline__ int padded_row(int x, int y, int z, int ny, int nz) {
     return ((x + 1) * (ny + 2) + (y + 1)) * (nz + 2) + (z + 1);
+}
+
+// 16-byte group of channels [8*plane, 8*plane + 8) of row v in plane-layout storage with R rows.
+template <class T>
+__device__ __forceinline__ T* plane_at(T* base, long long R, int plane, int v) {
+    return base + ((size_t)plane * R + v) * 8;
 }
 
 // Input features of voxel (x, y, z): scaled noisy map, log1p(mu_a), log1p(mu_s)/4, tissue state.
@@ -56,8 +62,8 @@ __device__ __forceinline__ void voxel_features(const float* a_noisy, const float
     f[3] = (fl & (BD_FLAG_ABLATED | BD_FLAG_VOID)) ? 0.f : ((fl & BD_FLAG_DRY) ? 0.5f : 1.f);
 }
 
-__global__ void k_unet_input(int nx, int ny, int nz, const float* a_noisy, const float4* props, const uint8_t* flags,
-                             float scale, __nv_bfloat16* x16, uint8_t* mask) {
+__global__ void k_unet_input(int nx, int ny, int nz, long long R, const float* a_noisy, const float4* props,
+                             const uint8_t* flags, float scale, __nv_bfloat16* x16, uint8_t* mask) {
     const long long n = (long long)nx * ny * nz;
     for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < n; u += (long long)gridDim.x * blockDim.x) {
         const int z = (int)(u % nz);
@@ -82,15 +88,15 @@ __global__ void k_unet_input(int nx, int ny, int nz, const float* a_noisy, const
         __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(q);
 #pragma unroll
         for (int f = 0; f < 8; ++f) h[f] = __floats2bfloat162_rn(v[2 * f], v[2 * f + 1]);
-        uint4* dst = reinterpret_cast<uint4*>(x16 + (size_t)padded_row(x, y, z, ny, nz) * 16);
-        dst[0] = q[0];
-        dst[1] = q[1];
+        const int row = padded_row(x, y, z, ny, nz);
+        *reinterpret_cast<uint4*>(plane_at(x16, R, 0, row)) = q[0];
+        *reinterpret_cast<uint4*>(plane_at(x16, R, 1, row)) = q[1];
     }
 }
 
 // Average (sum_mask == false) of the 8 children, or their sum gated by gate(coarse) > 0.
-__global__ void k_pool(int nxc, int nyc, int nzc, int C, const __nv_bfloat16* fine, const __nv_bfloat16* gate,
-                       __nv_bfloat16* coarse, int sum_mask) {
+__global__ void k_pool(int nxc, int nyc, int nzc, long long Rc, long long Rf, int C, const __nv_bfloat16* fine,
+                       const __nv_bfloat16* gate, __nv_bfloat16* coarse, int sum_mask) {
     const int chunks = C / 8;
     const long long n = (long long)nxc * nyc * nzc * chunks;
     const int nyf = 2 * nyc, nzf = 2 * nzc;
@@ -103,7 +109,7 @@ __global__ void k_pool(int nxc, int nyc, int nzc, int C, const __nv_bfloat16* fi
         float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         for (int c8 = 0; c8 < 8; ++c8) {
             const int fx = 2 * x + (c8 >> 2), fy = 2 * y + ((c8 >> 1) & 1), fz = 2 * z + (c8 & 1);
-            const uint4 q = *reinterpret_cast<const uint4*>(fine + (size_t)padded_row(fx, fy, fz, nyf, nzf) * C + ch * 8);
+            const uint4 q = *reinterpret_cast<const uint4*>(plane_at(fine, Rf, ch, padded_row(fx, fy, fz, nyf, nzf)));
             const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&q);
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
@@ -112,9 +118,9 @@ __global__ void k_pool(int nxc, int nyc, int nzc, int C, const __nv_bfloat16* fi
                 acc[2 * j + 1] += f.y;
             }
         }
-        const size_t row = (size_t)padded_row(x, y, z, nyc, nzc) * C + ch * 8;
+        const int vc = padded_row(x, y, z, nyc, nzc);
         if (sum_mask) {
-            const uint4 q = *reinterpret_cast<const uint4*>(gate + row);
+            const uint4 q = *reinterpret_cast<const uint4*>(plane_at(gate, Rc, ch, vc));
             const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&q);
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
@@ -130,22 +136,19 @@ __global__ void k_pool(int nxc, int nyc, int nzc, int C, const __nv_bfloat16* fi
         __nv_bfloat162* ho = reinterpret_cast<__nv_bfloat162*>(&o);
 #pragma unroll
         for (int j = 0; j < 4; ++j) ho[j] = __floats2bfloat162_rn(acc[2 * j], acc[2 * j + 1]);
-        *reinterpret_cast<uint4*>(coarse + row) = o;
+        *reinterpret_cast<uint4*>(plane_at(coarse, Rc, ch, vc)) = o;
     }
 }
 
-// out[c] += sum over all rows of g[row][c] (pad rows are zero).
-__global__ void k_bias_grad(long long rows, int C, const __nv_bfloat16* g, float* out) {
-    __shared__ float part[64];
-    for (int c = threadIdx.x; c < C; c += blockDim.x) part[c] = 0.f;
+// out[8*plane + j] += sum over the rows of plane blockIdx.y (pad and margin rows are zero).
+__global__ void k_bias_grad(long long R, const __nv_bfloat16* g, float* out) {
+    __shared__ float part[8];
+    if (threadIdx.x < 8) part[threadIdx.x] = 0.f;
     __syncthreads();
-    const int chunks = C / 8;
-    const long long stride = (long long)gridDim.x * blockDim.x;  // a multiple of chunks (8 | 256)
-    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const int ch = (int)(t0 % chunks);
+    const int plane = blockIdx.y;
     float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (long long i = t0; i < rows * chunks; i += stride) {
-        const uint4 q = *reinterpret_cast<const uint4*>(g + (size_t)(i / chunks) * C + ch * 8);
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < R; r += (long long)gridDim.x * blockDim.x) {
+        const uint4 q = *reinterpret_cast<const uint4*>(plane_at(g, R, plane, (int)r));
         const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&q);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -155,9 +158,13 @@ __global__ void k_bias_grad(long long rows, int C, const __nv_bfloat16* g, float
         }
     }
 #pragma unroll
-    for (int j = 0; j < 8; ++j) atomicAdd(&part[ch * 8 + j], acc[j]);
+    for (int j = 0; j < 8; ++j) {
+        float v = acc[j];
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&part[j], v);
+    }
     __syncthreads();
-    for (int c = threadIdx.x; c < C; c += blockDim.x) atomicAdd(&out[c], part[c]);
+    if (threadIdx.x < 8) atomicAdd(&out[plane * 8 + threadIdx.x], part[threadIdx.x]);
 }
 
 __global__ void k_adam(long long n, float* p, const float* g, float* m, float* v, float lr, float b1, float b2,
@@ -265,7 +272,8 @@ struct UnetImpl {
              cudaStream_t st) {
         const Level& L = lv[coarse];
         const long long n = (long long)L.nx * L.ny * L.nz * (C / 8);
-        k_pool<<<blocks_for(n), 256, 0, st>>>(L.nx, L.ny, L.nz, C, fine, gate, out, sum_mask ? 1 : 0);
+        k_pool<<<blocks_for(n), 256, 0, st>>>(L.nx, L.ny, L.nz, L.rows(), lv[coarse - 1].rows(), C, fine, gate, out,
+                                              sum_mask ? 1 : 0);
         BD_CHECK_LAUNCH("k_pool");
         return BD_OK;
     }
@@ -274,7 +282,8 @@ struct UnetImpl {
                 const float* target, float loss_norm, cudaStream_t st) {
         const Level& L0 = lv[0];
         const long long n0 = (long long)L0.nx * L0.ny * L0.nz;
-        k_unet_input<<<blocks_for(n0), 256, 0, st>>>(L0.nx, L0.ny, L0.nz, a_noisy, props, flags, scale, x16, mask);
+        k_unet_input<<<blocks_for(n0), 256, 0, st>>>(L0.nx, L0.ny, L0.nz, L0.rows(), a_noisy, props, flags, scale, x16,
+                                                     mask);
         BD_CHECK_LAUNCH("k_unet_input");
         int rc;
         if ((rc = conv(call(0, 0, BD_CONV_FWD_RELU, x16, a1), st))) return rc;
@@ -314,7 +323,8 @@ struct UnetImpl {
         const LayerSpec& s = kLayers[l];
         const Level& L = lv[level];
         if (int rc = wgrad_launch(L.nx, L.ny, L.nz, s.cin, s.cout, s.taps, g, x, grads + w_off[l], st, err)) return rc;
-        k_bias_grad<<<blocks_for(L.rows() * (s.cout / 8)), 256, 0, st>>>(L.rows(), s.cout, g, grads + b_off[l]);
+        const dim3 bg(std::max(1, std::min(blocks_for(L.rows()), 296)), s.cout / 8);
+        k_bias_grad<<<bg, 256, 0, st>>>(L.rows(), g, grads + b_off[l]);
         BD_CHECK_LAUNCH("k_bias_grad");
         return BD_OK;
     }

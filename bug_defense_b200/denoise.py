@@ -8,7 +8,7 @@ BF16 tensor-core convolutions with FP32 accumulation) that maps a map traced wit
 plus the optical properties and tissue state, to an estimate of the many-photon map. Plain MC stays
 the fallback and the judge of its error.
 
-Volumes on the device are channels-last bf16 rows with a one-voxel zero pad (see
+Volumes on the device are bf16 "8-channel planes" with a one-voxel zero pad (see
 include/bugdef.h, "Absorbed-map denoiser"). This module holds the layer-level wrappers of the C ABI
 (used by the tests and by the network driver) and the Denoiser / training front end.
 """
@@ -32,19 +32,33 @@ def _torch():
     return torch
 
 
-def to_padded(x, dtype=None):
-    """(C, nx, ny, nz) tensor -> contiguous (nx+2, ny+2, nz+2, C) bf16 tensor with a zero pad."""
+def plane_rows(nx: int, ny: int, nz: int) -> int:
+    """Rows per 8-channel plane of a level: padded rows plus the zero margin (bd_conv_plane_rows)."""
+    return int(_lib.load().bd_conv_plane_rows(int(nx), int(ny), int(nz)))
+
+
+def zeros_planes(channels: int, shape, device="cuda"):
+    """Zeroed plane-layout volume: (channels/8, R, 8) bf16."""
     torch = _torch()
-    dtype = dtype or torch.bfloat16
+    return torch.zeros((channels // 8, plane_rows(*shape), 8), dtype=torch.bfloat16, device=device)
+
+
+def to_planes(x):
+    """(C, nx, ny, nz) tensor -> plane-layout bf16 volume (C/8, R, 8) with a zero pad and margin."""
+    torch = _torch()
     c, nx, ny, nz = x.shape
-    out = torch.zeros((nx + 2, ny + 2, nz + 2, c), dtype=dtype, device=x.device)
-    out[1:-1, 1:-1, 1:-1, :] = x.permute(1, 2, 3, 0).to(dtype)
+    out = zeros_planes(c, (nx, ny, nz), x.device)
+    vol = out[:, :(nx + 2) * (ny + 2) * (nz + 2)].view(c // 8, nx + 2, ny + 2, nz + 2, 8)
+    vol[:, 1:-1, 1:-1, 1:-1, :] = x.reshape(c // 8, 8, nx, ny, nz).permute(0, 2, 3, 4, 1).to(torch.bfloat16)
     return out
 
 
-def from_padded(xp):
-    """(nx+2, ny+2, nz+2, C) -> (C, nx, ny, nz) float32 (interior only)."""
-    return xp[1:-1, 1:-1, 1:-1, :].permute(3, 0, 1, 2).float()
+def from_planes(t, shape):
+    """Plane-layout volume -> (C, nx, ny, nz) float32 (interior only)."""
+    nx, ny, nz = shape
+    cb = t.shape[0]
+    vol = t[:, :(nx + 2) * (ny + 2) * (nz + 2)].view(cb, nx + 2, ny + 2, nz + 2, 8)
+    return vol[:, 1:-1, 1:-1, 1:-1, :].permute(0, 4, 1, 2, 3).reshape(cb * 8, nx, ny, nz).float()
 
 
 def image_bytes(taps: int, k_channels: int, n_slice: int) -> int:
@@ -65,7 +79,7 @@ def pack_weights(w, taps, cin, cout, n_off=0, n_slice=None, transpose=False, str
 def conv3d(mode, inp, wimage, shape, cin, cout_total, n_slice=None, n_off=0, taps=27, bias=None, out=None,
            out_coarse=None, aux=None, aux2=None, head=None, stream=None, **head_args):
     """One convolution layer through bd_conv3d (synchronous). `shape` is the interior size of the
-    level the convolution runs on; tensors are padded channels-last bf16 (see to_padded)."""
+    level the convolution runs on; volumes are plane-layout bf16 (see to_planes)."""
     c = _lib.ConvCall()
     c.nx, c.ny, c.nz = shape
     c.cin, c.cout_total = cin, cout_total
@@ -178,3 +192,197 @@ def init_params(seed: int = 0):
         parts += [w.ravel(), np.zeros(co)]
     parts += [np.zeros(HEAD), np.zeros(1)]
     return np.concatenate(parts).astype(np.float32)
+
+
+# --------------------------------------------------------------------------- data, training, use
+
+SCALE = 1e4          # absorbed fraction per voxel -> network range (hot cuticle voxels ~1)
+LO_PHOTONS = 15_000
+HI_PHOTONS = 1_500_000
+
+
+def mc_map(sample: dict, n_photons: int, seed: int, props=None, stream=None):
+    """Absorbed map (fraction of launched weight per voxel, fp32 on the device) of `n_photons`
+    traced through a crater_sample geometry; returns (map, packed props, FP64 ledger)."""
+    torch = _torch()
+    from . import voxel_mc
+    nx, ny, nz = sample["shape"]
+    dev = sample["mu_a"].device
+    if props is None:
+        props = voxel_mc.pack_props(sample["mu_a"], sample["mu_s"], sample["g"], sample["n"], dev, stream=stream)
+    p = voxel_mc.make_params(Nx=nx, Ny=ny, Nz=nz, Lx=sample["Lx"], Ly=sample["Ly"], Lz=sample["Lz"],
+                             n_photons=n_photons, spot_dia=sample["spot_dia"],
+                             theta_inc_deg=sample["theta_inc_deg"], seed=seed, tally_fluence=False)
+    A = torch.zeros(nx * ny * nz, dtype=torch.float32, device=dev)
+    ledger = voxel_mc.trace(p, props, A, flags=sample["flags"], stream=stream)
+    A.mul_(1.0 / n_photons)
+    return A.view(nx, ny, nz), props, ledger
+
+
+def relative_l2(a, ref) -> float:
+    """||a - ref|| / ||ref|| over the whole map (FP64 sums)."""
+    a = a.double().flatten(); ref = ref.double().flatten()
+    return float(((a - ref).norm() / ref.norm()).item())
+
+
+def train(n_pairs: int = 2000, epochs: int = 2, shape=(200, 200, 128), lr: float = 1e-3, seed: int = 0,
+          lo: int = LO_PHOTONS, hi: int = HI_PHOTONS, params=None, log_every: int = 100, log=print):
+    """Train the denoiser on the GPU with its own kernels: for each of n_pairs random craters
+    (workloads.crater_sample, seeds seed*1e6 + i) trace a lo- and a hi-photon map with fresh MC
+    seeds every epoch, run forward + backward and one Adam step (cosine-decayed lr). Returns the
+    trained FP32 parameters (numpy) and a history of (step, mean loss)."""
+    torch = _torch()
+    from . import workloads
+    net = UNet(shape, training=True, params=params if params is not None else init_params(seed))
+    total = n_pairs * epochs
+    hist, acc, cnt, step = [], 0.0, 0, 0
+    for ep in range(epochs):
+        for i in range(n_pairs):
+            s = workloads.crater_sample(seed * 1_000_000 + i, *shape)
+            base = (seed * 1_000_003 + ep * 7919 + i) * 2
+            a_lo, props, _ = mc_map(s, lo, base)
+            a_hi, _, _ = mc_map(s, hi, base + 1, props=props)
+            net.forward_backward(a_lo, props, s["flags"], a_hi, scale=SCALE)
+            lr_t = lr * 0.5 * (1.0 + np.cos(np.pi * step / max(total, 1)))
+            net.adam(lr_t)
+            step += 1
+            if step % log_every == 0 or step == total:
+                acc += net.read_loss(); cnt += 1
+                hist.append((step, acc / cnt))
+                log(f"step {step}/{total} loss {acc / cnt:.5g}")
+                acc, cnt = 0.0, 0
+    out = net.params().cpu().numpy()
+    net.close()
+    return out, hist
+
+
+class Denoiser:
+    """Trained absorbed-map denoiser: `den(a_noisy, props, flags)` returns the denoised map.
+    Weights load from an .npz written by save(); the network is fully convolutional and runs on
+    any grid whose dims are multiples of 4."""
+
+    def __init__(self, params, scale: float = SCALE, meta: dict | None = None):
+        self.params = np.asarray(params, dtype=np.float32)
+        self.scale = float(scale)
+        self.meta = dict(meta or {})
+        self._nets = {}
+
+    @classmethod
+    def load(cls, path=None):
+        from pathlib import Path
+        p = Path(path) if path is not None else DEFAULT_WEIGHTS
+        if not p.exists():
+            raise FileNotFoundError(f"denoiser weights not found: {p}")
+        z = np.load(p, allow_pickle=False)
+        meta = {k: z[k].item() if z[k].ndim == 0 else z[k].tolist() for k in z.files if k not in ("params",)}
+        return cls(z["params"], float(z["scale"]) if "scale" in z.files else SCALE, meta)
+
+    def save(self, path, **meta):
+        np.savez_compressed(path, params=self.params, scale=np.float64(self.scale),
+                            **{k: np.asarray(v) for k, v in meta.items()})
+
+    def net(self, shape, device=None):
+        key = (tuple(shape), str(device))
+        if key not in self._nets:
+            self._nets[key] = UNet(shape, training=False, params=self.params, device=device)
+        return self._nets[key]
+
+    def __call__(self, a_noisy, props, flags=None, out=None, stream=None):
+        shape = tuple(a_noisy.shape) if a_noisy.dim() == 3 else None
+        if shape is None:
+            raise ValueError("a_noisy must be a (nx, ny, nz) device tensor")
+        return self.net(shape, a_noisy.device).forward(a_noisy, props, flags, scale=self.scale, out=out,
+                                                       stream=stream)
+
+
+def _default_weights():
+    from pathlib import Path
+    return Path(__file__).resolve().parent / "weights" / "denoiser.npz"
+
+
+DEFAULT_WEIGHTS = _default_weights()
+
+
+def main(argv=None):
+    import argparse
+    import json
+    import time
+    ap = argparse.ArgumentParser(description="train the absorbed-map denoiser on the GPU")
+    ap.add_argument("cmd", choices=["train", "evaluate"])
+    ap.add_argument("--pairs", type=int, default=2000)
+    ap.add_argument("--epochs", type=int, default=2)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--shape", type=int, nargs=3, default=[200, 200, 128])
+    ap.add_argument("--out", default=str(DEFAULT_WEIGHTS))
+    ap.add_argument("--log", default=None)
+    ap.add_argument("--samples", type=int, default=8)
+    a = ap.parse_args(argv)
+    if a.cmd == "evaluate":
+        res = evaluate(Denoiser.load(a.out), n_samples=a.samples)
+        print(json.dumps(res))
+        if a.log:
+            from pathlib import Path
+            Path(a.log).write_text(json.dumps(res, indent=1) + "\n")
+        return
+    t0 = time.time()
+    lines = []
+
+    def log(msg):
+        line = f"[{time.time() - t0:8.1f}s] {msg}"
+        print(line, flush=True)
+        lines.append(line)
+
+    params, hist = train(n_pairs=a.pairs, epochs=a.epochs, shape=tuple(a.shape), lr=a.lr, seed=a.seed, log=log)
+    from pathlib import Path
+    Path(a.out).parent.mkdir(parents=True, exist_ok=True)
+    Denoiser(params).save(a.out, shape=np.asarray(a.shape), pairs=a.pairs, epochs=a.epochs, lr=a.lr, seed=a.seed,
+                          lo_photons=LO_PHOTONS, hi_photons=HI_PHOTONS, train_seconds=time.time() - t0)
+    if a.log:
+        Path(a.log).write_text("\n".join(lines) + "\n" + json.dumps({"history": hist}) + "\n")
+
+
+if __name__ == "__main__":
+    main()
+
+
+def evaluate(den: "Denoiser", n_samples: int = 8, seed0: int = 900_000, ref_photons: int = 100_000_000,
+             lo: int = LO_PHOTONS, plain: int = 150_000, shape=(200, 200, 128), timing_reps: int = 10) -> dict:
+    """Held-out comparison on random craters (seeds seed0 + k): relative L2 against a ref_photons
+    map of the noisy lo-photon map, the denoised lo-photon map and the plain `plain`-photon map,
+    plus CUDA-event times of each path (MC of lo photons + network, MC of plain photons)."""
+    torch = _torch()
+    from . import workloads
+    rows = []
+    for k in range(n_samples):
+        s = workloads.crater_sample(seed0 + k, *shape)
+        ref, props, _ = mc_map(s, ref_photons, 7 * k + 1)
+        a_lo, _, _ = mc_map(s, lo, 7 * k + 2, props=props)
+        a_pl, _, _ = mc_map(s, plain, 7 * k + 3, props=props)
+        out = den(a_lo, props, s["flags"])
+        rows.append(dict(seed=seed0 + k, depth=s["depth"], noisy=relative_l2(a_lo, ref), denoised=relative_l2(out, ref),
+                         plain=relative_l2(a_pl, ref)))
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+        e0.record()
+        for _ in range(timing_reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / timing_reps
+
+    s = workloads.crater_sample(seed0, *shape)
+    a_lo, props, _ = mc_map(s, lo, 11)
+    out = torch.empty(shape, dtype=torch.float32, device=a_lo.device)
+    t_mc_lo = timed(lambda: mc_map(s, lo, 12, props=props))
+    t_net = timed(lambda: den(a_lo, props, s["flags"], out=out))
+    t_mc_plain = timed(lambda: mc_map(s, plain, 13, props=props))
+    mean = lambda key: float(np.mean([r[key] for r in rows]))
+    return dict(samples=rows, rel_l2_noisy=mean("noisy"), rel_l2_denoised=mean("denoised"), rel_l2_plain=mean("plain"),
+                ms_mc_lo=t_mc_lo, ms_net=t_net, ms_mc_plain=t_mc_plain,
+                ms_denoised_path=t_mc_lo + t_net, speedup_vs_plain=t_mc_plain / (t_mc_lo + t_net),
+                lo_photons=lo, plain_photons=plain, ref_photons=ref_photons, shape=list(shape))

@@ -140,3 +140,69 @@ def engine_kwargs(geo: dict) -> dict:
                 plume_closure=geo["plume_closure"], initial_dry_mask=geo["dry_mask"],
                 initial_ablated_mask=geo["ablated_mask"], air_gap_range=geo["air_gap_range"],
                 wavelength_nm=532.0, seed=geo["seed"] + 1)
+
+
+def crater_sample(seed: int, nx: int = 200, ny: int = 200, nz: int = 128, device=None) -> dict:
+    """One random crater geometry on the full-resolution stack (the denoiser's training and
+    evaluation inputs): layer properties drawn as for full_coupled_run, then a paraboloid crater of
+    depth U(0, 0.9) mm and radius U(0.08, 0.45) mm near the beam axis (none in 15% of samples) is
+    emptied (void optics, ablated + void flags), a charred rim of 0-3 voxels takes char optics and
+    the dry flag, and half of the craters hold a uniform plume absorption U(0, 1.5)/mm.
+    Built on the device with torch; returns fp32 optical grids, flag bytes and the beam geometry
+    (Gaussian 0.5 mm spot at 22 deg, centre of the face)."""
+    import torch
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    rng = np.random.default_rng(seed)
+    lay = _draw_layers(rng)
+    n_tissue = int(round(sum(t for _, t in STACK) * 1e-3 / DX))
+    n_air = nz - n_tissue
+    names = _layer_index(n_tissue, n_air)
+    zp = {key: np.zeros(nz) for key in ("mu_a", "mu_s", "g")}
+    zp["n"] = np.ones(nz)
+    abl_z = np.zeros(nz, bool)
+    dry_z = np.zeros(nz, bool)
+    for kk, nm in enumerate(names):
+        if nm == "top_air":
+            abl_z[kk] = True
+        elif nm != "below":
+            dry_z[kk] = "cuticle" in nm          # cuticle starts dry, as in full_coupled_run
+            for key in ("mu_a", "mu_s", "g", "n"):
+                zp[key][kk] = lay[nm][key]
+    shape = (nx, ny, nz)
+    grids = {k: torch.as_tensor(v, dtype=torch.float32, device=dev).expand(shape).contiguous() for k, v in zp.items()}
+    fz = np.where(abl_z, 0x05, 0) | np.where(dry_z, 0x02, 0)
+    flags = torch.as_tensor(fz.astype(np.uint8), device=dev).expand(shape).contiguous()
+    Lx, Ly = nx * DX, ny * DX
+    x = (torch.arange(nx, device=dev, dtype=torch.float32) + 0.5) * DX
+    y = (torch.arange(ny, device=dev, dtype=torch.float32) + 0.5) * DX
+    z = (torch.arange(nz, device=dev, dtype=torch.float32) + 0.5) * DX
+    z0 = n_air * DX
+    has = rng.random() >= 0.15
+    depth = float(rng.uniform(0.0, 0.9)) if has else 0.0
+    radius = float(rng.uniform(0.08, 0.45))
+    xc = Lx / 2 + float(rng.uniform(-0.1, 0.1))
+    yc = Ly / 2 + float(rng.uniform(-0.1, 0.1))
+    rim = int(rng.integers(0, 4))
+    plume = float(rng.uniform(0.0, 1.5)) if rng.random() < 0.5 else 0.0
+    char_mu_a, char_mu_s = float(rng.uniform(10, 30)), float(rng.uniform(10, 30))
+    r2 = ((x[:, None] - xc) ** 2 + (y[None, :] - yc) ** 2) / (radius * radius)
+    floor = z0 + depth * torch.clamp(1.0 - r2, min=0.0)                 # crater floor per column
+    zz = z[None, None, :]
+    crater = (zz < floor[:, :, None]) & (zz >= z0) & (r2[:, :, None] < 1.0) if depth > 0 else torch.zeros(
+        shape, dtype=torch.bool, device=dev)
+    if rim > 0 and depth > 0:
+        shell = (zz < floor[:, :, None] + rim * DX) & (zz >= z0) & (r2[:, :, None] < (1.0 + rim * DX / radius) ** 2)
+        shell &= ~crater & (grids["mu_s"] > 0)
+        grids["mu_a"][shell] = char_mu_a
+        grids["mu_s"][shell] = char_mu_s
+        grids["g"][shell] = 0.9
+        grids["n"][shell] = 1.56
+        flags[shell] |= 0x02
+    grids["mu_a"][crater] = plume
+    grids["mu_s"][crater] = 0.0
+    grids["g"][crater] = 0.8
+    grids["n"][crater] = 1.0
+    flags[crater] |= 0x05
+    return dict(shape=shape, Lx=Lx, Ly=Ly, Lz=nz * DX, mu_a=grids["mu_a"], mu_s=grids["mu_s"], g=grids["g"],
+                n=grids["n"], flags=flags, spot_dia=0.5, theta_inc_deg=22.0, depth=depth, radius=radius, rim=rim,
+                plume=plume, seed=seed)

@@ -318,9 +318,10 @@ BD_API int bd_engine_timing_read(BdEngine* e, double* stage_ms /* [4] */, int64_
  * No counterpart in the reference, which has no learned component; these are the building blocks
  * of the U-Net that denoises low-photon absorbed-power maps.
  *
- * Volumes are channels-last bf16 with a one-voxel zero pad: a level with interior nx x ny x nz
- * stores (nx+2)(ny+2)(nz+2) rows of `channels` values, z fastest, and every call keeps the pad
- * rows zero. Taps are ordered t = (dx+1)*9 + (dy+1)*3 + (dz+1) (27 taps) or t = (dx+1)*3 + (dy+1)
+ * Volumes are bf16 with a one-voxel zero pad, stored as 8-channel planes: a level with interior
+ * nx x ny x nz has R = bd_conv_plane_rows(nx, ny, nz) rows per plane ((nx+2)(ny+2)(nz+2) padded rows,
+ * z fastest, then a zero margin), and channel c of padded row v is element ((c/8)*R + v)*8 + c%8.
+ * Buffers must start zeroed; every call keeps the pad and margin rows zero. Taps are ordered t = (dx+1)*9 + (dy+1)*3 + (dz+1) (27 taps) or t = (dx+1)*3 + (dy+1)
  * (9 taps, for an input whose z neighbours are packed into its channels); weights are FP32
  * [taps][cout][cin]. */
 #define BD_CONV_FWD_RELU   0  /* out = relu(conv + bias) at this level                               */
@@ -337,10 +338,10 @@ typedef struct BdConvCall {
     int n_off, n_slice;      /* output channels [n_off, n_off + n_slice) computed by this call      */
     int taps;                /* 27 or 9                                                             */
     int mode;                /* BD_CONV_*                                                           */
-    const void* input;       /* bf16 padded input rows                                              */
+    const void* input;       /* bf16 input planes                                                   */
     const void* wimage;      /* weight image of this slice (bd_conv_pack_weights)                   */
     const float* bias;       /* [n_slice] (forward modes) or NULL                                   */
-    void* out;               /* bf16 padded output rows (finer level for the UPADD modes)           */
+    void* out;               /* bf16 output planes (finer level for the UPADD modes)                */
     void* out_coarse;        /* FWD_UPADD: optional copy of relu(conv + bias) at this level         */
     const void* aux;         /* see the modes above                                                 */
     const void* aux2;
@@ -356,9 +357,11 @@ typedef struct BdConvCall {
     const float* target;     /* fp32 [nx*ny*nz] or NULL (inference)                                 */
     float* head_grad;        /* [17], accumulated                                                   */
     double* loss;            /* [1], accumulated                                                    */
-    void* grad_out;          /* bf16 padded [.][16] gradient at the head input                      */
+    void* grad_out;          /* bf16 planes (16 channels): gradient at the head input               */
 } BdConvCall;
 
+/* Rows per 8-channel plane of a level (padded rows plus the zero margin the tile copies read). */
+BD_API int64_t bd_conv_plane_rows(int nx, int ny, int nz);
 /* Bytes of the shared-memory weight image of one output-channel slice. */
 BD_API int64_t bd_conv_image_bytes(int taps, int k_channels, int n_slice);
 /* FP32 [taps][cout][cin] -> bf16 image for output channels [n_off, n_off + n_slice). transpose=0:

@@ -33,12 +33,17 @@ def _dev(a, dtype=None):
 
 def _pad(a):
     from bug_defense_b200 import denoise
-    return denoise.to_padded(_dev(a))
+    return denoise.to_planes(_dev(a))
 
 
-def _unpad(t):
+def _unpad(t, shape=SHAPE):
     from bug_defense_b200 import denoise
-    return denoise.from_padded(t).double().cpu().numpy()
+    return denoise.from_planes(t, shape).double().cpu().numpy()
+
+
+def _zeros(channels, shape=SHAPE):
+    from bug_defense_b200 import denoise
+    return denoise.zeros_planes(channels, shape)
 
 
 def _close(got, ref, frac=1e-2):
@@ -63,13 +68,16 @@ def test_forward_relu_matches_oracle(gpu, cin, cout):
     w = _weights(rng, 27, cin, cout)
     b = _bf(rng.normal(0, 0.1, cout))
     img = denoise.pack_weights(_dev(w), 27, cin, cout)
-    out = torch.zeros((SHAPE[0] + 2, SHAPE[1] + 2, SHAPE[2] + 2, cout), dtype=torch.bfloat16, device="cuda")
+    out = _zeros(cout)
     denoise.conv3d(_lib.CONV_FWD_RELU, _pad(x), img, SHAPE, cin, cout, bias=_dev(b), out=out)
     ref = ou.relu(ou.conv(x, w) + b[:, None, None, None])
     _close(_unpad(out), ref)
-    # the pad rows stay zero
+    # the pad and margin rows stay zero
+    nxp, nyp, nzp = (s + 2 for s in SHAPE)
     o = out.float()
-    assert float(o[0].abs().max()) == 0.0 and float(o[:, :, -1].abs().max()) == 0.0
+    vol = o[:, :nxp * nyp * nzp].view(-1, nxp, nyp, nzp, 8)
+    assert float(vol[:, 0].abs().max()) == 0.0 and float(vol[:, :, :, -1].abs().max()) == 0.0
+    assert float(o[:, nxp * nyp * nzp:].abs().max()) == 0.0
 
 
 def test_forward_nine_taps_z_packed(gpu):
@@ -81,7 +89,7 @@ def test_forward_nine_taps_z_packed(gpu):
     w = _weights(rng, 9, 16, 16)
     w[:, :, 12:] = 0.0
     img = denoise.pack_weights(_dev(w), 9, 16, 16)
-    out = torch.zeros((SHAPE[0] + 2, SHAPE[1] + 2, SHAPE[2] + 2, 16), dtype=torch.bfloat16, device="cuda")
+    out = _zeros(16)
     denoise.conv3d(_lib.CONV_FWD_RELU, _pad(x16), img, SHAPE, 16, 16, taps=9, bias=_dev(np.zeros(16)), out=out)
     ref = ou.relu(ou.conv(x16, w, taps=9))
     _close(_unpad(out), ref)
@@ -100,7 +108,7 @@ def test_forward_output_slices_cover_64_by_64(gpu):
     x = _rand(rng, (64,) + SHAPE)
     w = _weights(rng, 27, 64, 64)
     b = _bf(rng.normal(0, 0.1, 64))
-    out = torch.zeros((SHAPE[0] + 2, SHAPE[1] + 2, SHAPE[2] + 2, 64), dtype=torch.bfloat16, device="cuda")
+    out = _zeros(64)
     xd, wd, bd = _pad(x), _dev(w), _dev(b)
     for off in (0, 32):
         img = denoise.pack_weights(wd, 27, 64, 64, n_off=off, n_slice=32)
@@ -121,7 +129,7 @@ def test_data_gradient_raw_and_masked(gpu, cin, cout):
     wd = _dev(w)
     slices = [(0, cin)] if not (cout == 64 and cin == 64) else [(0, 32), (32, 32)]
     for mode in (_lib.CONV_BWD_RAW, _lib.CONV_BWD_MASK):
-        out = torch.zeros((SHAPE[0] + 2, SHAPE[1] + 2, SHAPE[2] + 2, cin), dtype=torch.bfloat16, device="cuda")
+        out = _zeros(cin)
         for off, ns in slices:
             img = denoise.pack_weights(wd, 27, cin, cout, n_off=off, n_slice=ns, transpose=True)
             denoise.conv3d(mode, _pad(gy), img, SHAPE, cout, cin, n_slice=ns, n_off=off, out=out,
@@ -141,13 +149,13 @@ def test_upsampling_forward_adds_skip(gpu, cin, cout):
     w = _weights(rng, 27, cin, cout)
     b = _bf(rng.normal(0, 0.1, cout))
     img = denoise.pack_weights(_dev(w), 27, cin, cout)
-    out = torch.zeros((fine[0] + 2, fine[1] + 2, fine[2] + 2, cout), dtype=torch.bfloat16, device="cuda")
-    oc = torch.zeros((COARSE[0] + 2, COARSE[1] + 2, COARSE[2] + 2, cout), dtype=torch.bfloat16, device="cuda")
+    out = _zeros(cout, fine)
+    oc = _zeros(cout, COARSE)
     denoise.conv3d(_lib.CONV_FWD_UPADD, _pad(x), img, COARSE, cin, cout, bias=_dev(b), out=out, out_coarse=oc,
                    aux=_pad(skip))
     u = ou.relu(ou.conv(x, w) + b[:, None, None, None])
-    _close(_unpad(oc), u)
-    _close(_unpad(out), ou.up(u) + skip)
+    _close(_unpad(oc, COARSE), u)
+    _close(_unpad(out, fine), ou.up(u) + skip)
 
 
 @pytest.mark.parametrize("cin,cout", [(64, 32), (32, 16)])
@@ -163,10 +171,10 @@ def test_upsampling_gradient_adds_residual(gpu, cin, cout):
     resid = _rand(rng, (cout,) + fine)
     act = _rand(rng, (cout,) + fine, positive_frac=0.6)
     img = denoise.pack_weights(_dev(w), 27, cout, cin, transpose=True)
-    out = torch.zeros((fine[0] + 2, fine[1] + 2, fine[2] + 2, cout), dtype=torch.bfloat16, device="cuda")
+    out = _zeros(cout, fine)
     denoise.conv3d(_lib.CONV_BWD_UPADD, _pad(g), img, COARSE, cin, cout, out=out, aux=_pad(resid), aux2=_pad(act))
     dp = ou.conv_data_grad(g, w)
-    _close(_unpad(out), (resid + ou.up(dp) / 8.0) * (act > 0))
+    _close(_unpad(out, fine), (resid + ou.up(dp) / 8.0) * (act > 0))
 
 
 @pytest.mark.parametrize("train", [False, True])
@@ -186,7 +194,7 @@ def test_head_fuses_output_layer_and_loss(gpu, train):
     pred = torch.zeros(SHAPE, device="cuda")
     hg = torch.zeros(17, device="cuda")
     loss = torch.zeros(1, dtype=torch.float64, device="cuda")
-    gout = torch.zeros((SHAPE[0] + 2, SHAPE[1] + 2, SHAPE[2] + 2, 16), dtype=torch.bfloat16, device="cuda")
+    gout = _zeros(16)
     denoise.conv3d(_lib.CONV_FWD_HEAD, _pad(x), img, SHAPE, 16, 16, bias=_dev(b), head=_dev(head),
                    a_noisy=_dev(a_noisy), mask=_dev(mask, torch.uint8), scale=scale, loss_norm=norm, pred=pred,
                    target=_dev(target) if train else None, head_grad=hg if train else None,
