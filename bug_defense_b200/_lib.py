@@ -147,6 +147,10 @@ class EpochDiag(Structure):
                 ("void_zlimit", c_double)]
 
 
+TUNE_MC_BLOCKS_PER_SM = 0
+TUNE_STENCIL_XC = 1
+TUNE_PLUME_XC = 2
+
 CONV_FWD_RELU = 0
 CONV_FWD_UPADD = 1
 CONV_FWD_HEAD = 2
@@ -198,6 +202,8 @@ _SIGNATURES = {
     "bd_engine_set_mc": (c_int, [c_void_p, POINTER(McParams)]),
     "bd_engine_timing": (c_int, [c_void_p, c_int]),
     "bd_engine_timing_read": (c_int, [c_void_p, POINTER(c_double), POINTER(c_int64)]),
+    "bd_tune_set": (c_int, [c_int, c_int]),
+    "bd_tune_get": (c_int, [c_int, POINTER(c_int)]),
     "bd_conv_plane_rows": (c_int64, [c_int, c_int, c_int]),
     "bd_conv_image_bytes": (c_int64, [c_int, c_int, c_int]),
     "bd_conv_pack_weights": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),

@@ -15,6 +15,9 @@ namespace bd {
 void set_error(const char* fmt, ...);
 int fail(int code, const char* fmt, ...);
 int cuda_status(cudaError_t e, const char* what);
+// Launch-shape knobs (BD_TUNE_*) and the generation counter bumped by every change.
+int tune_value(int knob);
+int tune_generation();
 
 #define BD_CUDA(call)                                                   \
     do {                                                                \

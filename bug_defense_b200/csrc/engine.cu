@@ -16,6 +16,7 @@
 struct StageGraph {
     cudaGraphExec_t exec = nullptr;
     std::vector<unsigned char> key;
+    int tune_gen = -1;   // launch shapes baked into the graph
 };
 
 struct BdEngine {
@@ -52,7 +53,8 @@ static int run_stage(BdEngine* e, StageGraph& g, const void* key, size_t key_len
                      F enqueue) {
     if (!use_graph) return enqueue(st);
     const unsigned char* kb = static_cast<const unsigned char*>(key);
-    if (!g.exec || g.key.size() != key_len || (key_len && memcmp(g.key.data(), kb, key_len) != 0)) {
+    if (!g.exec || g.tune_gen != bd::tune_generation() || g.key.size() != key_len ||
+        (key_len && memcmp(g.key.data(), kb, key_len) != 0)) {
         graph_reset(g);
         cudaGraph_t graph = nullptr;
         BD_CUDA(cudaStreamBeginCapture(e->cap_stream, cudaStreamCaptureModeThreadLocal));
@@ -70,6 +72,7 @@ static int run_stage(BdEngine* e, StageGraph& g, const void* key, size_t key_len
             return bd::cuda_status(ce, "cudaGraphInstantiate");
         }
         g.key.assign(kb, kb + key_len);
+        g.tune_gen = bd::tune_generation();
     }
     BD_CUDA(cudaGraphLaunch(g.exec, st));
     return BD_OK;

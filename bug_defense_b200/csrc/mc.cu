@@ -523,7 +523,9 @@ int mc_launch(const BdMcParams* p, const float* props, const uint8_t* flags, flo
         per_sm[ax] = std::max(1, std::min(nb, 16));
         cudaGetLastError();
     }
-    int blocks = (int)std::min<long long>((p->n_photons + 127) / 128, (long long)sm_count * per_sm[ax]);
+    const int want = tune_value(BD_TUNE_MC_BLOCKS_PER_SM);
+    const int use_sm = want > 0 ? std::min(want, per_sm[ax]) : per_sm[ax];
+    int blocks = (int)std::min<long long>((p->n_photons + 127) / 128, (long long)sm_count * use_sm);
     blocks = std::max(1, std::min(blocks, max_blocks));
     BD_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st));
     BD_CUDA(cudaMemsetAsync(partials, 0, sizeof(double) * BD_LEDGER_LEN * blocks, st));

@@ -498,10 +498,6 @@ static Geo make_geo(int nx, int ny, int nz, float dx, float dy, float dz, float 
     return g;
 }
 
-#ifndef BD_STENCIL_XC
-#define BD_STENCIL_XC 8
-#endif
-
 template <int MODE, int BC, bool ARR, bool CHAR>
 static void launch_substeps(const Geo& g, const AblConst& c, float* Ta, float* Tb, int n, const float* src,
                             const float* K, const float* R, const uint8_t* F, float* H, float* Om, float* Chi,
@@ -514,7 +510,7 @@ static void launch_substeps(const Geo& g, const AblConst& c, float* Ta, float* T
                      make_tmap_3d_f32(&mb, Tb, g.nx, g.ny, g.nz, ST_PZ, ST_PY, 1) &&
                      make_tmap_3d_f32(&mk, K, g.nx, g.ny, g.nz, ST_PZ, ST_PY, 1);
     if (tma) {
-        const int xc = BD_STENCIL_XC;
+        const int xc = tune_value(BD_TUNE_STENCIL_XC);
         const dim3 grid((g.nz + ST_BZ - 1) / ST_BZ, (g.ny + ST_BY - 1) / ST_BY, (g.nx + xc - 1) / xc);
         for (int s = 0; s < n; ++s) {
             float* out = (s & 1) ? Ta : Tb;
@@ -641,10 +637,6 @@ int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, floa
     return fail(BD_ERR_INVALID_ARG, "bd_ablation_advance: bad bc_mode %d", p->bc_mode);
 }
 
-#ifndef BD_PLUME_XC
-#define BD_PLUME_XC 4
-#endif
-
 int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
                  cudaStream_t st, const int* zlimit, int full_first, uint8_t* mask, int* err) {
     int steps;
@@ -668,7 +660,7 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
 #endif
     const bool tma = err != nullptr && make_tmap_3d_f32(&map_a, Ca, p->nx, p->ny, p->nz, PL_PZ, PL_PY, 1) &&
                      make_tmap_3d_f32(&map_b, Cb, p->nx, p->ny, p->nz, PL_PZ, PL_PY, 1);
-    const int xc = BD_PLUME_XC;
+    const int xc = tune_value(BD_TUNE_PLUME_XC);
     const dim3 tgrid((p->nz + PL_BZ - 1) / PL_BZ, (p->ny + PL_BY - 1) / PL_BY, (p->nx + xc - 1) / xc);
     const long long total = (long long)steps * n_substeps;
     for (long long s = 0; s < total; ++s) {

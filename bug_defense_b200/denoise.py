@@ -342,9 +342,6 @@ def main(argv=None):
         Path(a.log).write_text("\n".join(lines) + "\n" + json.dumps({"history": hist}) + "\n")
 
 
-if __name__ == "__main__":
-    main()
-
 
 def evaluate(den: "Denoiser", n_samples: int = 8, seed0: int = 900_000, ref_photons: int = 100_000_000,
              lo: int = LO_PHOTONS, plain: int = 150_000, shape=(200, 200, 128), timing_reps: int = 10) -> dict:
@@ -386,3 +383,7 @@ def evaluate(den: "Denoiser", n_samples: int = 8, seed0: int = 900_000, ref_phot
                 ms_mc_lo=t_mc_lo, ms_net=t_net, ms_mc_plain=t_mc_plain,
                 ms_denoised_path=t_mc_lo + t_net, speedup_vs_plain=t_mc_plain / (t_mc_lo + t_net),
                 lo_photons=lo, plain_photons=plain, ref_photons=ref_photons, shape=list(shape))
+
+
+if __name__ == "__main__":
+    main()

@@ -313,6 +313,18 @@ BD_API int bd_engine_set_mc(BdEngine* e, const BdMcParams* mc);
 BD_API int bd_engine_timing(BdEngine* e, int enable);
 BD_API int bd_engine_timing_read(BdEngine* e, double* stage_ms /* [4] */, int64_t* epochs);
 
+/* ---- launch-shape tuning ------------------------------------------------------------------------
+ * No counterpart in the reference (its kernels have fixed launch shapes). Process-wide knobs read at
+ * every launch; results do not depend on them beyond the order of FP32 atomic tally additions. A
+ * change bumps a generation counter so engines re-capture their epoch graphs. */
+#define BD_TUNE_MC_BLOCKS_PER_SM  0  /* persistent MC grid: 128-thread CTAs per SM, 1..16 (0 = occupancy
+                                        limit); photons per thread = n_photons / (grid * 128)          */
+#define BD_TUNE_STENCIL_XC        1  /* x-planes per CTA of the TMA substep kernel, 1..64 (default 8)   */
+#define BD_TUNE_PLUME_XC          2  /* x-planes per CTA of the TMA plume kernel, 1..64 (default 4)     */
+#define BD_TUNE_COUNT             3
+BD_API int bd_tune_set(int knob, int value);
+BD_API int bd_tune_get(int knob, int* value);
+
 /* ---------------------------------------------------------------------------------------------
  * Absorbed-map denoiser: 3-D convolution layers (tcgen05 BF16 tensor cores, FP32 accumulation).
  * No counterpart in the reference, which has no learned component; these are the building blocks
