@@ -15,6 +15,13 @@ namespace bd {
 void set_error(const char* fmt, ...);
 int fail(int code, const char* fmt, ...);
 int cuda_status(cudaError_t e, const char* what);
+// Absorbed-weight tallies are 64-bit fixed point: weight * 2^36 per deposit, rounded to nearest.
+// Integer sums are exact and independent of the order of the atomic additions (FP32 sums of
+// millions of deposits lose the small ones once the voxel total dwarfs them). A photon deposits at
+// most its weight (<= 1 plus rare roulette gains), so 2^26 photons per launch keep every voxel sum
+// below 2^62.
+constexpr float kTallyScale = 68719476736.0f;          // 2^36
+constexpr long long kTallyMaxPhotons = 1LL << 26;
 // Launch-shape knobs (BD_TUNE_*) and the generation counter bumped by every change.
 int tune_value(int knob);
 int tune_generation();

@@ -29,6 +29,7 @@ struct BdEngine {
     bd::EngineDyn* dyn_host = nullptr; // pinned
     unsigned long long* queue = nullptr;
     double* partials = nullptr;
+    unsigned long long* tally64 = nullptr;   // fixed-point absorbed-weight tally of the MC stage
     int partial_blocks = 0;
     int sm_count = 148;
     long long epochs_enqueued = 0;  // host mirror of the epoch count (photon-stream offsets)
@@ -178,6 +179,8 @@ static int validate(const BdEngineDesc* d) {
     BD_REQUIRE(d->A != nullptr, "bd_engine_create: absorbed map A is required");
     BD_REQUIRE(d->voxel_volume > 0.0, "bd_engine_create: voxel_volume must be > 0");
     BD_REQUIRE((long long)p.nx * p.ny * p.nz < (1LL << 31), "bd_engine_create: grid exceeds 2^31 voxels");
+    BD_REQUIRE(d->mc.n_photons >= 0 && d->mc.n_photons <= kTallyMaxPhotons,
+               "bd_engine_create: photons per epoch must be 0..%lld", (long long)kTallyMaxPhotons);
     return BD_OK;
 }
 
@@ -199,6 +202,9 @@ extern "C" int bd_engine_create(const BdEngineDesc* desc, BdEngine** out) {
     if (err == cudaSuccess) err = cudaMallocHost(&e->dyn_host, sizeof(EngineDyn));
     if (err == cudaSuccess) err = cudaMalloc(&e->queue, sizeof(unsigned long long));
     if (err == cudaSuccess) err = cudaMalloc(&e->partials, sizeof(double) * BD_LEDGER_LEN * e->partial_blocks);
+    const size_t nv_all = (size_t)desc->phase.nx * desc->phase.ny * desc->phase.nz;
+    if (err == cudaSuccess) err = cudaMalloc(&e->tally64, sizeof(unsigned long long) * nv_all);
+    if (err == cudaSuccess) err = cudaMemset(e->tally64, 0, sizeof(unsigned long long) * nv_all);
     if (err == cudaSuccess) err = cudaMemset(e->dyn, 0, sizeof(EngineDyn));
     for (int q = 0; q < 4 && err == cudaSuccess; ++q) err = cudaEventCreate(&e->ev[q]);
     if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->cap_stream, cudaStreamNonBlocking);
@@ -230,6 +236,7 @@ extern "C" int bd_engine_destroy(BdEngine* e) {
     cudaFreeHost(e->dyn_host);
     cudaFree(e->queue);
     cudaFree(e->partials);
+    cudaFree(e->tally64);
     for (int q = 0; q < 4; ++q)
         if (e->ev[q]) cudaEventDestroy(e->ev[q]);
     for (cudaEvent_t ev : e->ring) cudaEventDestroy(ev);
@@ -277,7 +284,7 @@ extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void*
             BD_CUDA(cudaMemsetAsync(d.A, 0, sizeof(float) * nv, s));
             if (d.L && (d.mc.options & BD_MC_TALLY_FLUENCE)) BD_CUDA(cudaMemsetAsync(d.L, 0, sizeof(float) * nv, s));
             return mc_launch(&mp, d.phase.props, d.phase.flags, d.A, d.L, d.lat_depth, e->dyn->ledger, e->queue,
-                             e->partials, e->partial_blocks, e->sm_count, s, &e->dyn->mc_offset);
+                             e->partials, e->partial_blocks, e->sm_count, s, &e->dyn->mc_offset, e->tally64);
         });
         if (rc) return rc;
     }
@@ -327,6 +334,8 @@ extern "C" int bd_engine_set_mc(BdEngine* e, const BdMcParams* mc) {
     BD_REQUIRE(e && mc, "bd_engine_set_mc: NULL argument");
     BD_REQUIRE(mc->nx == e->d.phase.nx && mc->ny == e->d.phase.ny && mc->nz == e->d.phase.nz,
                "bd_engine_set_mc: grid differs from the engine's");
+    BD_REQUIRE(mc->n_photons >= 0 && mc->n_photons <= kTallyMaxPhotons,
+               "bd_engine_set_mc: photons per epoch must be 0..%lld", (long long)kTallyMaxPhotons);
     e->d.mc = *mc;
     return BD_OK;
 }

@@ -58,6 +58,6 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
 int plume_policy_steps(const BdPlumeParams* p, int* n_steps, float* dt_step, float* decay_step);
 int mc_launch(const BdMcParams* p, const float* props, const uint8_t* flags, float* A, float* L, double* latz,
               double* ledger, unsigned long long* queue, double* partials, int max_blocks, int sm_count,
-              cudaStream_t st, const long long* offset_dev);
+              cudaStream_t st, const long long* offset_dev, unsigned long long* tally64);
 
 }  // namespace bd

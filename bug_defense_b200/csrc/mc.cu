@@ -154,8 +154,8 @@ struct ThreadLedger {
 template <int DEPTH>  // 2: launch along +z at z=0 ; 0: launch along +x at x=0
 __device__ __forceinline__ void trace_photon(const McDev& P, long long pid, const float4* __restrict__ props,
                                              const uint8_t* __restrict__ flags, float* __restrict__ A,
-                                             float* __restrict__ L, double* __restrict__ latz,
-                                             double* sl, ThreadLedger& tl) {
+                                             unsigned long long* __restrict__ A64, float* __restrict__ L,
+                                             double* __restrict__ latz, double* sl, ThreadLedger& tl) {
     PhotonRng rng;
     rng.init(P.seed, (unsigned long long)(P.offset + pid));
     const bool metal = (P.options & BD_MC_METAL_SEMANTICS) != 0;
@@ -256,7 +256,8 @@ __device__ __forceinline__ void trace_photon(const McDev& P, long long pid, cons
             {
                 const float dw = w * pr.y;
                 const float w_new = w - dw;
-                atomicAdd(&A[idx], dw);
+                if (A64) atomicAdd(&A64[idx], __float2ull_rn(dw * kTallyScale));
+                else atomicAdd(&A[idx], dw);
                 const double lost = (double)w - (double)w_new;  // exact: both are FP32 values
                 if (flags != nullptr && (__ldg(&flags[idx]) & BD_FLAG_ABLATED)) atomicAdd(&sl[BD_LEDGER_ABSORBED_VOID], lost);
                 else tl.absorbed += lost;
@@ -361,6 +362,7 @@ done:
 template <int DEPTH>
 __global__ void __launch_bounds__(128, BD_MC_MIN_BLOCKS) k_mc_trace(McDev P, const float4* __restrict__ props,
                                                      const uint8_t* __restrict__ flags, float* __restrict__ A,
+                                                     unsigned long long* __restrict__ A64,
                                                      float* __restrict__ L, double* __restrict__ latz,
                                                      unsigned long long* __restrict__ queue,
                                                      double* __restrict__ partials,
@@ -376,7 +378,7 @@ __global__ void __launch_bounds__(128, BD_MC_MIN_BLOCKS) k_mc_trace(McDev P, con
     for (;;) {
         unsigned long long p = atomicAdd(queue, 1ull);
         if (p >= N) break;
-        trace_photon<DEPTH>(P, (long long)p, props, flags, A, L, latz, sl, tl);
+        trace_photon<DEPTH>(P, (long long)p, props, flags, A, A64, L, latz, sl, tl);
     }
     // warp reduction of the per-thread channels, one FP64 atomic per warp and channel
     double v0 = tl.absorbed;
@@ -428,6 +430,18 @@ __global__ void k_pack_props(const float* __restrict__ mu_a, const float* __rest
     }
 }
 
+// A[i] += fixed-point tally[i] in weight units; the tally is left zeroed for the next launch.
+__global__ void k_tally_finalize(unsigned long long* __restrict__ t64, float* __restrict__ A, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long v = t64[i];
+        if (v != 0ull) {
+            A[i] += (float)((double)v * (1.0 / (double)kTallyScale));
+            t64[i] = 0ull;
+        }
+    }
+}
+
 __global__ void k_fold(float* __restrict__ src, double* __restrict__ dst, long long n) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
@@ -445,6 +459,8 @@ __global__ void k_fold(float* __restrict__ src, double* __restrict__ dst, long l
 struct BdMcContext {
     unsigned long long* queue = nullptr;
     double* partials = nullptr;
+    unsigned long long* tally64 = nullptr;   // fixed-point absorbed tally, grown to the largest grid
+    long long tally_cap = 0;
     int partial_blocks = 0;
     int device = -1;
     int sm_count = 148;
@@ -474,6 +490,7 @@ extern "C" int bd_mc_destroy(BdMcContext* c) {
     if (!c) return BD_OK;
     cudaFree(c->queue);
     cudaFree(c->partials);
+    cudaFree(c->tally64);
     delete c;
     return BD_OK;
 }
@@ -512,7 +529,7 @@ McDev mc_dev_params(const BdMcParams* p) {
 // Launch with caller-provided scratch (queue counter + per-block partials).
 int mc_launch(const BdMcParams* p, const float* props, const uint8_t* flags, float* A, float* L,
               double* latz, double* ledger, unsigned long long* queue, double* partials, int max_blocks,
-              int sm_count, cudaStream_t st, const long long* offset_dev) {
+              int sm_count, cudaStream_t st, const long long* offset_dev, unsigned long long* tally64) {
     McDev d = mc_dev_params(p);
     static int per_sm[2] = {0, 0};
     const int ax = p->launch_axis == 0 ? 0 : 1;
@@ -531,10 +548,15 @@ int mc_launch(const BdMcParams* p, const float* props, const uint8_t* flags, flo
     BD_CUDA(cudaMemsetAsync(partials, 0, sizeof(double) * BD_LEDGER_LEN * blocks, st));
     const float4* pr = reinterpret_cast<const float4*>(props);
     if (p->launch_axis == 0)
-        k_mc_trace<2><<<blocks, 128, 0, st>>>(d, pr, flags, A, L, latz, queue, partials, offset_dev);
+        k_mc_trace<2><<<blocks, 128, 0, st>>>(d, pr, flags, A, tally64, L, latz, queue, partials, offset_dev);
     else
-        k_mc_trace<0><<<blocks, 128, 0, st>>>(d, pr, flags, A, L, latz, queue, partials, offset_dev);
+        k_mc_trace<0><<<blocks, 128, 0, st>>>(d, pr, flags, A, tally64, L, latz, queue, partials, offset_dev);
     BD_CHECK_LAUNCH("k_mc_trace");
+    if (tally64) {
+        const long long nv = (long long)p->nx * p->ny * p->nz;
+        k_tally_finalize<<<grid_for(nv, 256), 256, 0, st>>>(tally64, A, nv);
+        BD_CHECK_LAUNCH("k_tally_finalize");
+    }
     k_ledger_reduce<<<1, 32, 0, st>>>(partials, blocks, (double)p->n_photons, ledger);
     BD_CHECK_LAUNCH("k_ledger_reduce");
     return BD_OK;
@@ -548,8 +570,20 @@ extern "C" int bd_mc_trace(BdMcContext* c, const BdMcParams* p, const float* pro
     if (rc) return rc;
     BD_REQUIRE(props != nullptr && A != nullptr && ledger != nullptr, "bd_mc_trace: props, A and ledger are required");
     BD_REQUIRE(!(p->options & BD_MC_TALLY_FLUENCE) || L != nullptr, "bd_mc_trace: BD_MC_TALLY_FLUENCE needs L");
+    BD_REQUIRE(p->n_photons <= kTallyMaxPhotons,
+               "bd_mc_trace: at most %lld photons per launch (fixed-point tally range); split into batches",
+               (long long)kTallyMaxPhotons);
+    const long long nv = (long long)p->nx * p->ny * p->nz;
+    if (nv > c->tally_cap) {
+        cudaFree(c->tally64);
+        c->tally64 = nullptr;
+        c->tally_cap = 0;
+        BD_CUDA(cudaMalloc(&c->tally64, sizeof(unsigned long long) * nv));
+        BD_CUDA(cudaMemset(c->tally64, 0, sizeof(unsigned long long) * nv));
+        c->tally_cap = nv;
+    }
     return mc_launch(p, props, flags, A, L, lat_depth, ledger, c->queue, c->partials, c->partial_blocks,
-                     c->sm_count, as_stream(stream), nullptr);
+                     c->sm_count, as_stream(stream), nullptr, c->tally64);
 }
 
 extern "C" int bd_mc_pack_props(const float* mu_a, const float* mu_s, const float* g, const float* n,
@@ -636,5 +670,5 @@ extern "C" int bd_mc_trace_noalloc(const BdMcParams* p, const float* props, cons
     double* partials = reinterpret_cast<double*>(static_cast<unsigned char*>(base) + MC_NOALLOC_QUEUE_BYTES);
     // mc_launch zeroes the queue counter and the ledger rows it uses before the kernel runs
     return mc_launch(p, props, flags, A, L, lat_depth, ledger, queue, partials, MC_NOALLOC_MAX_BLOCKS, sms,
-                     as_stream(stream), nullptr);
+                     as_stream(stream), nullptr, nullptr);
 }

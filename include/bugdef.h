@@ -189,7 +189,9 @@ BD_API int bd_mc_trace(BdMcContext* ctx, const BdMcParams* p, const float* props
  * looks up that device's copy of the array, so make it before any timing-critical phase.
  * Launches needing more than 2048 blocks are rejected with BD_ERR_INVALID_ARG. Every call
  * shares the array: calls that overlap on the GPU (other streams, other host threads on the
- * same device) race and must be serialised by the caller. Results equal bd_mc_trace's. */
+ * same device) race and must be serialised by the caller. Its absorbed map is summed with FP32
+ * atomics (bd_mc_trace sums exactly in 64-bit fixed point, which needs per-voxel scratch): the
+ * same photon histories, with FP32 rounding of the per-voxel sums (~1e-5 relative at 1e5 photons). */
 BD_API int bd_mc_trace_noalloc(const BdMcParams* p, const float* props, const uint8_t* flags, float* A, float* L,
                                double* lat_depth, double* ledger, void* stream);
 /* dst64[i] += src32[i]; src32[i] = 0 (folds a batch tally into an FP64 accumulator). */

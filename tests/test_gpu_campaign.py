@@ -1,0 +1,94 @@
+"""Launch-shape knobs and the batched campaign on the GPU.
+
+Absorbed-weight tallies are exact 64-bit fixed point and every other kernel is deterministic, so
+neither the launch shapes nor running instances concurrently may change a single bit."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _knob(k, v=None):
+    import ctypes
+    from bug_defense_b200 import _lib
+    if v is None:
+        out = ctypes.c_int(0)
+        _lib.call("bd_tune_get", k, ctypes.byref(out))
+        return out.value
+    _lib.call("bd_tune_set", k, int(v))
+
+
+@pytest.fixture
+def restore_knobs(gpu):
+    from bug_defense_b200 import _lib
+    keep = {k: _knob(k) for k in (_lib.TUNE_MC_BLOCKS_PER_SM, _lib.TUNE_STENCIL_XC, _lib.TUNE_PLUME_XC)}
+    yield
+    for k, v in keep.items():
+        _knob(k, v)
+
+
+def test_knob_validation(gpu, restore_knobs):
+    from bug_defense_b200 import _lib
+    with pytest.raises(ValueError):
+        _knob(_lib.TUNE_STENCIL_XC, 0)
+    with pytest.raises(ValueError):
+        _knob(_lib.TUNE_MC_BLOCKS_PER_SM, 17)
+    with pytest.raises(ValueError):
+        _knob(7, 1)
+
+
+def test_launch_shapes_leave_results_bit_identical(gpu, restore_knobs):
+    from bug_defense_b200 import _lib, thermal
+    rng = np.random.default_rng(5)
+    n = (24, 20, 36)
+    T0 = 25 + 50 * rng.random(n); Q = rng.random(n) * 1e-3
+    K = 1e-4 + 5e-4 * rng.random(n); R = 2e-3 + 2e-3 * rng.random(n)
+    outs = []
+    for xc in (4, 8, 16):
+        _knob(_lib.TUNE_STENCIL_XC, xc)
+        outs.append(thermal.run_thermal3d_substeps_gpu(T0, Q, K, R, *n, 0.015, 0.015, 0.015, 5e-5, 9, h_eff=2e-5,
+                                                       t_ambient=25.0, is_active=1))
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+    cube = {k: np.full((16, 16, 20), v) for k, v in (("mu_a", 2.0), ("mu_s", 15.0), ("g", 0.85), ("n", 1.4))}
+    kw = dict(n_photons=60_000, base_seed=77, Lx=0.24, Ly=0.24, Lz=0.3, Nx=16, Ny=16, Nz=20, custom_3d_props=cube,
+              spot_dia=0.1)
+    maps = []
+    for blocks in (0, 2, 5):
+        _knob(_lib.TUNE_MC_BLOCKS_PER_SM, blocks)
+        maps.append(gpu.run_voxel_mc3d(**kw)["A_3d"])
+    assert np.array_equal(maps[0], maps[1]) and np.array_equal(maps[0], maps[2])
+
+
+def _small(index, photons=20_000):
+    from bug_defense_b200 import campaign
+    inst = campaign.campaign_instances(1, grid=(24, 24, 128), n_plume_air=8)[index]
+    return dict(inst, n_photons=photons, pulse_ms=12.0)
+
+
+def test_concurrent_campaign_equals_instances_run_alone(gpu, restore_knobs):
+    import torch
+    from bug_defense_b200 import campaign
+    insts = [_small(i) for i in (1, 10, 23)]           # 532, 1064 and 2940 nm
+    camp = campaign.Campaign(insts)
+    camp.run(30, sync_every=10)
+    together = [(e.T.copy(), e.ablated.copy(), e.H_acc.copy()) for e in camp.engines]
+    for inst, (T, abl, H) in zip(insts, together):
+        solo = campaign.Campaign([inst])
+        solo.run(30, sync_every=30)
+        e = solo.engines[0]
+        assert np.array_equal(e.T, T) and np.array_equal(e.ablated, abl) and np.array_equal(e.H_acc, H)
+    # the lasers did work: every instance heated up, the 2940 nm one ablated
+    assert all(float(T.max()) > 40.0 for T, _, _ in together)
+    assert together[2][1].sum() > together[0][1].sum()
+
+
+def test_autotune_sets_the_fastest_candidates(gpu, restore_knobs):
+    from bug_defense_b200 import _lib, campaign
+    res = campaign.autotune(_small(4), epochs_per_trial=2,
+                            candidates={_lib.TUNE_MC_BLOCKS_PER_SM: [2, 4], _lib.TUNE_STENCIL_XC: [4, 8],
+                                        _lib.TUNE_PLUME_XC: [2, 4]})
+    for name, knob in (("mc_ctas_per_sm", _lib.TUNE_MC_BLOCKS_PER_SM), ("stencil_xc", _lib.TUNE_STENCIL_XC),
+                       ("plume_xc", _lib.TUNE_PLUME_XC)):
+        trials = res["trials"][name]
+        assert [v for v, _ in trials] == sorted(v for v, _ in trials) and all(t > 0 for _, t in trials)
+        assert res[name] == min(trials, key=lambda t: t[1])[0] == _knob(knob)

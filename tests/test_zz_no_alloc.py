@@ -49,8 +49,9 @@ def test_noalloc_entry_point_matches_allocating_one_on_two_calls(gpu):
         # same photon streams: counts identical, FP64 weights equal up to summation order
         np.testing.assert_array_equal(a[[0, 10, 11, 12]], b[[0, 10, 11, 12]])
         np.testing.assert_allclose(b, a, rtol=1e-12, atol=1e-9)
-        # FP32 atomic tallies: equal up to the order of the additions
-        np.testing.assert_allclose(A1.cpu().numpy(), A0.cpu().numpy(), rtol=1e-5, atol=1e-6)
+        # the same photon histories; this entry point sums the absorbed map with FP32 atomics while
+        # bd_mc_trace sums it exactly in fixed point, so the maps differ by FP32 rounding of the sums
+        np.testing.assert_allclose(A1.cpu().numpy(), A0.cpu().numpy(), rtol=1e-4, atol=1e-6)
         np.testing.assert_allclose(L1.cpu().numpy(), L0.cpu().numpy(), rtol=1e-5, atol=1e-6)
         np.testing.assert_allclose(z1.cpu().numpy(), z0.cpu().numpy(), rtol=1e-12, atol=1e-9)
 
