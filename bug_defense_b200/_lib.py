@@ -147,6 +147,17 @@ class EpochDiag(Structure):
                 ("void_zlimit", c_double)]
 
 
+class RecordSpec(Structure):
+    _fields_ = [("y", c_int32), ("k_surface", c_int32), ("band_k0", c_int32 * 3), ("band_k1", c_int32 * 3),
+                ("gap_k0", c_int32), ("gap_k1", c_int32), ("q_scale", c_float), ("plume_ratio_a", c_float)]
+
+
+class RecordHead(Structure):
+    _fields_ = [("time_s", c_double), ("epoch", c_double), ("plume_tau", c_double), ("n_new", c_double),
+                ("n_void", c_double), ("absorbed_weight", c_double), ("peak_T", c_float * 3),
+                ("depth_voxels", c_int32)]
+
+
 TUNE_MC_BLOCKS_PER_SM = 0
 TUNE_STENCIL_XC = 1
 TUNE_PLUME_XC = 2
@@ -202,6 +213,10 @@ _SIGNATURES = {
     "bd_engine_set_mc": (c_int, [c_void_p, POINTER(McParams)]),
     "bd_engine_timing": (c_int, [c_void_p, c_int]),
     "bd_engine_timing_read": (c_int, [c_void_p, POINTER(c_double), POINTER(c_int64)]),
+    "bd_engine_set_plume_optics": (c_int, [c_void_p, c_float, c_float, c_float, c_float]),
+    "bd_engine_refresh_props": (c_int, [c_void_p, c_void_p]),
+    "bd_record_slot_bytes": (c_int64, [c_int, c_int]),
+    "bd_engine_record": (c_int, [c_void_p, POINTER(RecordSpec), c_void_p, c_void_p]),
     "bd_tune_set": (c_int, [c_int, c_int]),
     "bd_tune_get": (c_int, [c_int, POINTER(c_int)]),
     "bd_conv_plane_rows": (c_int64, [c_int, c_int, c_int]),

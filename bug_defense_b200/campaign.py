@@ -147,11 +147,12 @@ def _stage_ms(eng, n_epochs: int, laser: bool) -> np.ndarray:
     return np.array(ms[:]) / max(int(n.value), 1)
 
 
-def autotune(inst: dict, epochs_per_trial: int = 6, candidates=None, device=None, log=None) -> dict:
-    """Pick the launch shapes for a campaign by timing them on a throwaway engine of `inst`:
-    MC CTAs per SM (photons per thread) on laser-on epochs, and x-planes per CTA of the fused
-    substep and plume kernels. Sets the winning values process-wide (bd_tune_set) and returns the
-    choices with every trial's per-epoch stage time (ms)."""
+def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=None) -> dict:
+    """Pick launch shapes by timing them on a throwaway engine of the real workload: `inst` is a
+    campaign instance dict or a callable returning an engine with a `laser_power` attribute.
+    Tries MC CTAs per SM (photons per thread) on laser-on epochs and x-planes per CTA of the
+    fused substep and plume kernels; sets the winning values process-wide (bd_tune_set) and
+    returns the choices with every trial's per-epoch stage time (ms)."""
     from . import _lib
     cand = dict(candidates or {})
     cand.setdefault(_lib.TUNE_MC_BLOCKS_PER_SM, [2, 4, 6, 8])
@@ -160,7 +161,7 @@ def autotune(inst: dict, epochs_per_trial: int = 6, candidates=None, device=None
     stage = {_lib.TUNE_MC_BLOCKS_PER_SM: 0, _lib.TUNE_STENCIL_XC: 1, _lib.TUNE_PLUME_XC: 2}
     names = {_lib.TUNE_MC_BLOCKS_PER_SM: "mc_ctas_per_sm", _lib.TUNE_STENCIL_XC: "stencil_xc",
              _lib.TUNE_PLUME_XC: "plume_xc"}
-    eng = make_engine(inst, device=device)
+    eng = inst() if callable(inst) else make_engine(inst, device=device)
     eng.step_epochs(3)                       # warm-up: graphs, caches, a first crater
     out = {"trials": {}}
     for knob, values in cand.items():

@@ -229,10 +229,14 @@ class CoupledAblationEngine:
         ph.t_abl = self.t_abl
         ph.alpha_max_stable = self.alpha_max_stable
         ph.k_void, ph.rho_cp_void, ph.t_void = self.k_void, self.rho_cp_void, self.t_void
+        self._ds_t = {}
         if self.dry_state is not None:
             for key, fld in (('mu_a', 'ds_mu_a'), ('mu_s', 'ds_mu_s'), ('g', 'ds_g'), ('n', 'ds_n'), ('k', 'ds_k'),
                              ('rho_cp', 'ds_rho_cp'), ('t_remove', 'ds_t_remove')):
-                setattr(ph, fld, self._gref(self._ds_value(key, self._opt_t)))
+                ref = self._gref(self._ds_value(key, self._opt_t))
+                if ref.ptr:
+                    self._ds_t[key] = self._keep[-1]
+                setattr(ph, fld, ref)
         cs = self.char_state
         ph.has_char_state = int(cs is not None)
         ph.cs_chi_remove = 1.0
@@ -324,6 +328,37 @@ class CoupledAblationEngine:
         if getattr(self, '_handle', None):
             mp = self._mc_params()
             _lib.call("bd_engine_set_mc", self._handle, ctypes.byref(mp))
+
+    def switch_wavelength(self, wavelength_nm: float, optical: dict = None, dry_state: dict = None,
+                          power: float = None):
+        """Mid-run wavelength switch of the dual-wavelength runner
+        (run_dual_permutation_suite.py:254-283): intact (non-ablated) voxels take the new optical
+        properties and dry-state optics, the wet copies restart from the current optics, the plume
+        takes the new wavelength's extinction constants (plume.py:270-278) and re-derives its
+        extinction; the packed MC properties follow before the next epoch. Arrays are full grids."""
+        intact = ((self._flags & _lib.FLAG_ABLATED) == 0)
+        if optical is not None:
+            for key in ('mu_a', 'mu_s', 'g', 'n'):
+                new = to_dev(optical[key], self.dev).reshape(self.shape)
+                self._opt_t[key].copy_(torch.where(intact, new, self._opt_t[key]))
+        if dry_state is not None and self.dry_state is not None:
+            for key in ('mu_a', 'mu_s', 'g', 'n'):
+                if key in dry_state and key in self._ds_t:
+                    t = self._ds_t[key].view(self.shape)
+                    t.copy_(torch.where(intact, to_dev(dry_state[key], self.dev).reshape(self.shape), t))
+        if self._wet is not None:
+            self._wet[0].view(self.shape).copy_(self._opt_t['mu_a'])
+            self._wet[1].view(self.shape).copy_(self._k)
+            self._wet[2].view(self.shape).copy_(self._rho)
+        if self.plume is not None:
+            self.plume.set_wavelength(wavelength_nm)
+            pl = self.plume
+            _lib.call("bd_engine_set_plume_optics", self._handle, float(pl.mu_max), float(pl.ratio_a),
+                      float(pl.ratio_s), float(pl.delta_mu))
+        self.wavelength_nm = float(wavelength_nm)
+        if power is not None:
+            self.power = power
+        _lib.call("bd_engine_refresh_props", self._handle, _lib.stream_ptr())
 
     def step_epoch(self, absorbed_map=None) -> dict:
         """Advance one coupled epoch; returns the diagnostics of coupled_ablation.py:605-617.

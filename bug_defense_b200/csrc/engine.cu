@@ -319,7 +319,7 @@ extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void*
         if (rc) return rc;
     }
     mark(e, st, 2);
-    rc = run_stage(e, e->g_end, nullptr, 0, graphs, st, [&](cudaStream_t s) -> int {
+    rc = run_stage(e, e->g_end, &e->pa, sizeof(e->pa), graphs, st, [&](cudaStream_t s) -> int {
         return phase_launch(e->pa, BD_PHASE_FULL, s);
     });
     if (e->timed) cudaEventRecord(e->ev[3], st);
@@ -328,6 +328,38 @@ extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void*
         if (ev) cudaEventRecord(ev, st);
     }
     return rc;
+}
+
+extern "C" int bd_engine_record(BdEngine* e, const BdRecordSpec* s, void* slot, void* stream) {
+    BD_REQUIRE(e && s && slot, "bd_engine_record: NULL argument");
+    const BdPhaseDesc& p = e->d.phase;
+    BD_REQUIRE(s->y >= 0 && s->y < p.ny, "bd_engine_record: slice y=%d outside 0..%d", s->y, p.ny - 1);
+    BD_REQUIRE(s->k_surface >= 0 && s->k_surface <= p.nz, "bd_engine_record: bad k_surface");
+    BD_REQUIRE(((uintptr_t)slot & 15) == 0, "bd_engine_record: slot must be 16-byte aligned");
+    RecordArgs a{};
+    a.nx = p.nx; a.ny = p.ny; a.nz = p.nz; a.y = s->y; a.k_surface = s->k_surface;
+    a.gap_k0 = s->gap_k0; a.gap_k1 = s->gap_k1;
+    for (int b = 0; b < 3; ++b) { a.band_k0[b] = s->band_k0[b]; a.band_k1[b] = s->band_k1[b]; }
+    a.q_scale = s->q_scale; a.plume_ratio_a = s->plume_ratio_a;
+    a.T = p.T; a.H = p.H_acc; a.chi = p.chi; a.A = e->d.A; a.flags = p.flags;
+    a.mu_ext = p.has_plume ? p.mu_ext : nullptr;
+    return record_launch(a, e->dyn, e->d.plume.dz, slot, as_stream(stream));
+}
+
+extern "C" int bd_engine_set_plume_optics(BdEngine* e, float mu_max, float ratio_a, float ratio_s, float delta_mu) {
+    BD_REQUIRE(e != nullptr, "bd_engine_set_plume_optics: NULL engine");
+    BD_REQUIRE(e->d.phase.has_plume, "bd_engine_set_plume_optics: engine has no plume");
+    BD_REQUIRE(mu_max >= 0.f && ratio_a >= 0.f && ratio_s >= 0.f && delta_mu >= 0.f,
+               "bd_engine_set_plume_optics: values must be >= 0");
+    e->d.phase.plume_mu_max = mu_max; e->d.phase.plume_ratio_a = ratio_a;
+    e->d.phase.plume_ratio_s = ratio_s; e->d.phase.plume_delta_mu = delta_mu;
+    e->pa.mu_max = mu_max; e->pa.ratio_a = ratio_a; e->pa.ratio_s = ratio_s; e->pa.delta_mu = delta_mu;
+    return BD_OK;
+}
+
+extern "C" int bd_engine_refresh_props(BdEngine* e, void* stream) {
+    BD_REQUIRE(e != nullptr, "bd_engine_refresh_props: NULL engine");
+    return phase_launch(e->pa, BD_PHASE_PROPS, as_stream(stream));
 }
 
 extern "C" int bd_engine_set_mc(BdEngine* e, const BdMcParams* mc) {

@@ -37,6 +37,7 @@ struct PhaseArgs {
     int has_plume;
     float t_abl, alpha_max, cs_chi_rem, k_void, rho_void, t_void;
     float delta_mu, mu_max, ratio_a, ratio_s, g_plume;
+    int props_only;
     float *T, *H, *chi, *mu_a, *mu_s, *g, *n, *k, *rho, *T_peak, *ablation_time;
     const float *h_lat, *wet_mu_a, *wet_k, *wet_rho;
     GridRef ds_mu_a, ds_mu_s, ds_g, ds_n, ds_k, ds_rho, ds_t_rem;
@@ -50,12 +51,25 @@ struct PhaseArgs {
 
 #define BD_PHASE_FULL 0  // phase update + removal + breach + void/plume/props pass
 #define BD_PHASE_INIT 1  // breach check (gap_open) + void/plume/props pass only
+#define BD_PHASE_PROPS 2 // void bits, plume extinction and packed MC properties only (no injection,
+                         // no diagnostics): after the optics change mid-run
 int phase_launch(const PhaseArgs& a, int mode, cudaStream_t st);
 int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, float* H, float* Om, float* Chi,
                     const uint8_t* F, const float* src, const float* K, const float* R, cudaStream_t st, int* err);
 int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
                  cudaStream_t st, const int* zlimit, int full_first, uint8_t* mask, int* err);
 int plume_policy_steps(const BdPlumeParams* p, int* n_steps, float* dt_step, float* decay_step);
+// Per-epoch xz recording (record.cu): inputs of one launch.
+struct RecordArgs {
+    int nx, ny, nz, y, k_surface, gap_k0, gap_k1;
+    int band_k0[3], band_k1[3];
+    float q_scale, plume_ratio_a;
+    const float *T, *H, *chi, *A, *mu_ext;
+    const uint8_t* flags;
+};
+constexpr int64_t kRecordHeadBytes = 256;   // BdRecordHead, padded so the slices stay aligned
+int record_launch(const RecordArgs& a, const EngineDyn* dyn, float plume_dz, void* slot, cudaStream_t st);
+
 int mc_launch(const BdMcParams* p, const float* props, const uint8_t* flags, float* A, float* L, double* latz,
               double* ledger, unsigned long long* queue, double* partials, int max_blocks, int sm_count,
               cudaStream_t st, const long long* offset_dev, unsigned long long* tally64);

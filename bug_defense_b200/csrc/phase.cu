@@ -140,7 +140,7 @@ __global__ void k_gap_breach(PhaseArgs a) {
 __global__ void __launch_bounds__(256) k_void_plume(PhaseArgs a, long long nv) {
     __shared__ double shd[8];
     const bool gap_open = a.gap_k0 > 0 && a.dyn->gap_open != 0;
-    const bool inject = a.dyn->n_new > 0;
+    const bool inject = !a.props_only && a.dyn->n_new > 0;
     const int mid_col = (a.nx / 2) * a.ny + a.ny / 2;
     double tau_sum = 0.0, abl_sum = 0.0, abl_cnt = 0.0;
     float peak = 0.0f;
@@ -194,6 +194,7 @@ __global__ void __launch_bounds__(256) k_void_plume(PhaseArgs a, long long nv) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
     if ((threadIdx.x & 31) == 0 && kmax >= 0) atomicMax(&a.dyn->void_zlimit, kmax + 1);
+    if (a.props_only) return;              // the epoch's diagnostics are already complete
     __shared__ float shp[8];
     if ((threadIdx.x & 31) == 0) shp[threadIdx.x >> 5] = peak;
     __syncthreads();
@@ -209,9 +210,16 @@ __global__ void __launch_bounds__(256) k_void_plume(PhaseArgs a, long long nv) {
     }
 }
 
-int phase_launch(const PhaseArgs& a, int mode, cudaStream_t st) {
+int phase_launch(const PhaseArgs& args, int mode, cudaStream_t st) {
+    PhaseArgs a = args;
+    a.props_only = mode == BD_PHASE_PROPS ? 1 : 0;
     const long long nv = (long long)a.nx * a.ny * a.nz;
     const int blocks = grid_for(nv, 256, 148 * 16);
+    if (mode == BD_PHASE_PROPS) {
+        k_void_plume<<<blocks, 256, 0, st>>>(a, nv);
+        BD_CHECK_LAUNCH("k_void_plume");
+        return BD_OK;
+    }
     if (mode == BD_PHASE_FULL) {
         k_phase_remove<<<blocks, 256, 0, st>>>(a, nv);
         BD_CHECK_LAUNCH("k_phase_remove");

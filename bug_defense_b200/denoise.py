@@ -210,11 +210,16 @@ def mc_map(sample: dict, n_photons: int, seed: int, props=None, stream=None):
     dev = sample["mu_a"].device
     if props is None:
         props = voxel_mc.pack_props(sample["mu_a"], sample["mu_s"], sample["g"], sample["n"], dev, stream=stream)
-    p = voxel_mc.make_params(Nx=nx, Ny=ny, Nz=nz, Lx=sample["Lx"], Ly=sample["Ly"], Lz=sample["Lz"],
-                             n_photons=n_photons, spot_dia=sample["spot_dia"],
-                             theta_inc_deg=sample["theta_inc_deg"], seed=seed, tally_fluence=False)
     A = torch.zeros(nx * ny * nz, dtype=torch.float32, device=dev)
-    ledger = voxel_mc.trace(p, props, A, flags=sample["flags"], stream=stream)
+    ledger = torch.zeros(_lib.LEDGER_LEN, dtype=torch.float64, device=dev)
+    done = 0
+    while done < n_photons:          # launches of at most 2^24 photons (exact fixed-point tallies)
+        nb = min(1 << 24, n_photons - done)
+        p = voxel_mc.make_params(Nx=nx, Ny=ny, Nz=nz, Lx=sample["Lx"], Ly=sample["Ly"], Lz=sample["Lz"],
+                                 n_photons=nb, spot_dia=sample["spot_dia"], theta_inc_deg=sample["theta_inc_deg"],
+                                 seed=seed, tally_fluence=False, photon_offset=done)
+        ledger += voxel_mc.trace(p, props, A, flags=sample["flags"], stream=stream)
+        done += nb
     A.mul_(1.0 / n_photons)
     return A.view(nx, ny, nz), props, ledger
 

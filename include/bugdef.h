@@ -312,8 +312,40 @@ BD_API int bd_engine_set_mc(BdEngine* e, const BdMcParams* mc);
 #define BD_STAGE_SUBSTEPS   1
 #define BD_STAGE_PLUME      2
 #define BD_STAGE_EPOCH_END  3
+/* Mid-run optics change, as the dual-wavelength runner switches lambda
+ * (knowledge/beetle/scripts/run_dual_permutation_suite.py:254-283): new plume extinction constants
+ * (plume.py:270-278), then, after the caller has written the new optical grids, a pass that
+ * re-derives the plume extinction and the packed MC properties (no plume injection, no change to
+ * the epoch's diagnostics). */
+BD_API int bd_engine_set_plume_optics(BdEngine* e, float mu_max, float ratio_a, float ratio_s, float delta_mu);
+BD_API int bd_engine_refresh_props(BdEngine* e, void* stream);
 BD_API int bd_engine_timing(BdEngine* e, int enable);
 BD_API int bd_engine_timing_read(BdEngine* e, double* stage_ms /* [4] */, int64_t* epochs);
+
+/* ---- per-epoch recording on the device ----------------------------------------------------------
+ * What the production runner pulls from the engine after every epoch
+ * (knowledge/beetle/scripts/run_highres_knowledge_suite.py:271-306): the xz slice at y of T, Q,
+ * the 4-phase map of compute_phase_map (simulation/run_multispectral_matrix.py:168-192, with the
+ * air gap as phase 3), the plume absorption, the crater depth below k_surface in that slice, the
+ * peak temperature of three depth bands, and the epoch's diagnostics. bd_engine_record enqueues
+ * the kernels that fill a record slot in device memory (no synchronisation); the caller copies the
+ * slot to pinned host memory asynchronously. Slot layout: BdRecordHead, padded to 256 bytes, then
+ * float T[nx][nz], float Q[nx][nz] (W/mm^3), float plume_mu_a[nx][nz], uint8 phase[nx][nz]. */
+typedef struct BdRecordSpec {
+    int32_t y;                         /* slice index                                               */
+    int32_t k_surface;                 /* first slice below the ambient air (crater depth origin)   */
+    int32_t band_k0[3], band_k1[3];    /* z ranges [k0, k1) of the peak temperatures                */
+    int32_t gap_k0, gap_k1;            /* air-gap slices (gap_k0 == gap_k1: none)                   */
+    float q_scale;                     /* W/mm^3 per unit of raw absorbed weight (0: laser off)     */
+    float plume_ratio_a;               /* mu_a share of the saturated plume extinction              */
+} BdRecordSpec;
+typedef struct BdRecordHead {
+    double time_s, epoch, plume_tau, n_new, n_void, absorbed_weight;
+    float peak_T[3];                   /* -inf for an empty band                                    */
+    int32_t depth_voxels;              /* 1 + deepest ablated slice below k_surface in the slice; 0 */
+} BdRecordHead;
+BD_API int64_t bd_record_slot_bytes(int nx, int nz);
+BD_API int bd_engine_record(BdEngine* e, const BdRecordSpec* spec, void* slot, void* stream);
 
 /* ---- launch-shape tuning ------------------------------------------------------------------------
  * No counterpart in the reference (its kernels have fixed launch shapes). Process-wide knobs read at

@@ -53,10 +53,11 @@ def test_version_and_errors_without_gpu(lib):
 
 
 STRUCTS = ["BdMcParams", "BdThermalParams", "BdAblationParams", "BdPlumeParams", "BdGridRef", "BdPhaseDesc",
-           "BdEngineDesc", "BdEpochDiag", "BdConvCall"]
+           "BdEngineDesc", "BdEpochDiag", "BdConvCall", "BdRecordSpec", "BdRecordHead"]
 PY = {"BdMcParams": "McParams", "BdThermalParams": "ThermalParams", "BdAblationParams": "AblationParams",
       "BdPlumeParams": "PlumeParams", "BdGridRef": "GridRef", "BdPhaseDesc": "PhaseDesc",
-      "BdEngineDesc": "EngineDesc", "BdEpochDiag": "EpochDiag", "BdConvCall": "ConvCall"}
+      "BdEngineDesc": "EngineDesc", "BdEpochDiag": "EpochDiag", "BdConvCall": "ConvCall",
+      "BdRecordSpec": "RecordSpec", "BdRecordHead": "RecordHead"}
 
 
 def test_struct_layouts_match_header():
