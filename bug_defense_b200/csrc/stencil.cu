@@ -358,23 +358,27 @@ __global__ void __launch_bounds__(TZ * TY) k_plume_step(int nx, int ny, int nz, 
 
 // TMA-staged plume step: a CTA owns a 32 (z) x 16 (y) column tile and marches a chunk of x
 // planes. Each plane's tile with a one-voxel y halo and a four-voxel z halo (40 x 18 floats, the
-// z start kept 16-byte aligned) is copied into a 4-stage shared-memory ring by the TMA engine,
-// three planes ahead of the one being computed, so every neighbour read comes from shared
-// memory and no thread waits on a global load chain.
-constexpr int PL_BZ = 32, PL_BY = 16, PL_PZ = PL_BZ + 8, PL_PY = PL_BY + 2, PL_STAGES = 4;
+// z start kept 16-byte aligned) is copied into a 6-stage shared-memory ring by the TMA engine,
+// four planes ahead of the one being computed, so every neighbour read comes from shared memory.
+// A thread owns 4 y rows of one z lane (128 threads per CTA) and one thread waits on the copies:
+// branches, barriers and barrier polls (a narrow pipe on sm_100) are paid once per plane for four
+// voxels per thread instead of two.
+constexpr int PL_BZ = 32, PL_BY = 16, PL_PZ = PL_BZ + 8, PL_PY = PL_BY + 2, PL_STAGES = 6;
+constexpr int PL_TY = 4, PL_RY = PL_BY / PL_TY;
 constexpr unsigned PL_TILE_BYTES = PL_PZ * PL_PY * sizeof(float);
 // each stage starts on a 128-byte boundary (TMA shared-memory destination alignment)
 constexpr int PL_STRIDE = ((PL_PZ * PL_PY * (int)sizeof(float) + 127) / 128) * 128 / (int)sizeof(float);
 static_assert(PL_STRIDE * sizeof(float) % 128 == 0, "stage stride must keep 128-byte alignment");
 static_assert(PL_STRIDE >= PL_PZ * PL_PY, "stage too small");
 
-__global__ void __launch_bounds__(TZ * TY) k_plume_step_tma(const __grid_constant__ CUtensorMap in_map,
-                                                            float* __restrict__ Cn, const uint8_t* __restrict__ M,
-                                                            int nx, int ny, int nz, int xc, PlumeConst c,
-                                                            const int* __restrict__ zlimit, int full_write,
-                                                            int* __restrict__ err) {
+__global__ void __launch_bounds__(TZ * PL_TY) k_plume_step_tma(const __grid_constant__ CUtensorMap in_map,
+                                                               float* __restrict__ Cn, const uint8_t* __restrict__ M,
+                                                               int nx, int ny, int nz, int xc, PlumeConst c,
+                                                               const int* __restrict__ zlimit, int full_write,
+                                                               int* __restrict__ err) {
     __shared__ __align__(128) float ring[PL_STAGES][PL_STRIDE];
     __shared__ __align__(8) unsigned long long bar[PL_STAGES];
+    __shared__ int s_fail;
     const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
     const int k0 = blockIdx.x * PL_BZ;
     const int j0 = blockIdx.y * PL_BY;
@@ -382,17 +386,17 @@ __global__ void __launch_bounds__(TZ * TY) k_plume_step_tma(const __grid_constan
     const int ie = min(nx, ib + xc);
     if (k0 >= zl || ib >= ie) return;  // uniform over the CTA
     const int tid = threadIdx.y * TZ + threadIdx.x;
+    const int nplanes = ie - ib + 2;  // planes ib-1 .. ie; load index q = plane - (ib - 1)
     if (tid == 0) {
         for (int q = 0; q < PL_STAGES; ++q) mbar_init(&bar[q], 1);
         mbar_init_fence();
-    }
-    __syncthreads();
-    const int nplanes = ie - ib + 2;  // planes ib-1 .. ie; q = plane - (ib - 1)
-    if (tid == 0) {
-        for (int q = 0; q < PL_STAGES && q < nplanes; ++q) {
+        s_fail = 0;
+        // loads 0 .. PL_STAGES-2 now; load q + PL_STAGES - 2 is issued at iteration q
+        for (int q = 0; q < PL_STAGES - 1 && q < nplanes; ++q) {
             mbar_expect_tx(&bar[q], PL_TILE_BYTES);
             tma_load_3d(ring[q], &in_map, k0 - 4, j0 - 1, ib - 1 + q, &bar[q]);
         }
+        if (!mbar_wait(&bar[0], 0) || !mbar_wait(&bar[1], 0)) s_fail = 1;
     }
     // Folded FTCS weights: C' = decay * (w0 c0 + wx (cw+ce) + wy (cs+cn) + wb cb + wt ct),
     // the same update as plume.py:73-79 with the products distributed.
@@ -402,62 +406,58 @@ __global__ void __launch_bounds__(TZ * TY) k_plume_step_tma(const __grid_constan
     const int plane = ny * nz;
     const int k = k0 + threadIdx.x;
     const bool kin = k < zl;
-    const int jr0 = j0 + threadIdx.y, jr1 = j0 + threadIdx.y + TY;
-    const bool row0 = kin && jr0 < ny, row1 = kin && jr1 < ny;
-    // the mask bytes of the next plane are fetched one iteration ahead of their use
-    uint8_t m0 = 0, m1 = 0;
-    if (row0) m0 = __ldg(&M[ib * plane + jr0 * nz + k]);
-    if (row1) m1 = __ldg(&M[ib * plane + jr1 * nz + k]);
-    bool ok = mbar_wait(&bar[0], 0);
-    ok = mbar_wait(&bar[1], 0) && ok;
+    bool act[PL_RY];
+    uint8_t m[PL_RY];
+#pragma unroll
+    for (int r = 0; r < PL_RY; ++r) {
+        const int j = j0 + threadIdx.y + r * PL_TY;
+        act[r] = kin && j < ny;
+        m[r] = act[r] ? __ldg(&M[ib * plane + j * nz + k]) : 0;   // next plane's bytes fetched a plane ahead
+    }
     for (int i = ib; i < ie; ++i) {
         const int q = i - ib + 1;
-        uint8_t n0 = 0, n1 = 0;
-        if (i + 1 < ie) {
-            if (row0) n0 = __ldg(&M[(i + 1) * plane + jr0 * nz + k]);
-            if (row1) n1 = __ldg(&M[(i + 1) * plane + jr1 * nz + k]);
+        uint8_t nm[PL_RY];
+#pragma unroll
+        for (int r = 0; r < PL_RY; ++r)
+            nm[r] = (act[r] && i + 1 < ie) ? __ldg(&M[(i + 1) * plane + (j0 + threadIdx.y + r * PL_TY) * nz + k]) : 0;
+        if (tid == 0 && !s_fail && !mbar_wait(&bar[(q + 1) % PL_STAGES], ((q + 1) / PL_STAGES) & 1)) s_fail = 1;
+        __syncthreads();  // load q+1 landed (seen by thread 0); every thread is done with plane i-2's stage
+        if (tid == 0 && q + PL_STAGES - 2 < nplanes) {
+            const int sl = (q + PL_STAGES - 2) % PL_STAGES;
+            fence_proxy_async_smem();
+            mbar_expect_tx(&bar[sl], PL_TILE_BYTES);
+            tma_load_3d(ring[sl], &in_map, k0 - 4, j0 - 1, ib - 1 + q + PL_STAGES - 2, &bar[sl]);
         }
-        ok = mbar_wait(&bar[(q + 1) % PL_STAGES], ((q + 1) / PL_STAGES) & 1) && ok;
         const float* tm = ring[(q - 1) % PL_STAGES];
         const float* tc = ring[q % PL_STAGES];
         const float* tp = ring[(q + 1) % PL_STAGES];
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
+        for (int r = 0; r < PL_RY; ++r) {
             // branch-free: every lane evaluates the stencil (its tile indices are always inside the
             // shared-memory stage), the mask byte selects neighbours and the result, and a single
             // predicated store writes void voxels only
-            const bool active = r == 0 ? row0 : row1;
-            const uint8_t m = r == 0 ? m0 : m1;
-            const int jy = threadIdx.y + r * TY;
+            const uint8_t mr = m[r];
+            const int jy = threadIdx.y + r * PL_TY;
             const int t = (jy + 1) * PL_PZ + threadIdx.x + 4;
             const float c0 = tc[t];
-            const float w = (m & 0x01) ? tm[t] : c0;
-            const float e = (m & 0x02) ? tp[t] : c0;
-            const float sx = (m & 0x04) ? tc[t - PL_PZ] : c0;
-            const float nn = (m & 0x08) ? tc[t + PL_PZ] : c0;
-            const float b = (m & 0x10) ? tc[t - 1] : c0;
-            const float tt = (m & 0x20) ? tc[t + 1] : c0;
+            const float w = (mr & 0x01) ? tm[t] : c0;
+            const float e = (mr & 0x02) ? tp[t] : c0;
+            const float sx = (mr & 0x04) ? tc[t - PL_PZ] : c0;
+            const float nn = (mr & 0x08) ? tc[t + PL_PZ] : c0;
+            const float b = (mr & 0x10) ? tc[t - 1] : c0;
+            const float tt = (mr & 0x20) ? tc[t + 1] : c0;
             float v = fmaxf((w0 * c0 + wx * (w + e) + wy * (sx + nn) + wb * b + wt * tt) * c.decay, 0.0f);
-            v = (m & BD_PM_UPDATE) ? v : 0.0f;
-            if (active && ((m & BD_PM_VOID) || full_write)) Cn[i * plane + (j0 + jy) * nz + k] = v;
-        }
-        m0 = n0;
-        m1 = n1;
-        __syncthreads();  // every thread is done with plane i-1's stage
-        if (tid == 0 && q + 3 < nplanes) {
-            const int s = (q + 3) % PL_STAGES;
-            fence_proxy_async_smem();
-            mbar_expect_tx(&bar[s], PL_TILE_BYTES);
-            tma_load_3d(ring[s], &in_map, k0 - 4, j0 - 1, i + 3, &bar[s]);
+            v = (mr & BD_PM_UPDATE) ? v : 0.0f;
+            if (act[r] && ((mr & BD_PM_VOID) || full_write)) Cn[i * plane + (j0 + jy) * nz + k] = v;
+            m[r] = nm[r];
         }
     }
-    if (!ok) {
+    __syncthreads();
+    if (tid == 0 && s_fail) {
         atomicExch(err, 1);
-        // drain: give any copy still in flight a bounded chance to land before the CTA exits
-        for (int q = 0; q < PL_STAGES; ++q) {
-            const int last = nplanes - 1 - ((nplanes - 1 - q) % PL_STAGES + PL_STAGES) % PL_STAGES;
-            if (last >= 0) mbar_wait(&bar[q], (last / PL_STAGES) & 1);
-        }
+        // drain: every copy issued gets a bounded chance to land before the CTA exits
+        const int last = min(nplanes, nplanes - 2 + PL_STAGES - 1);
+        for (int q = max(0, last - PL_STAGES); q < last; ++q) mbar_wait(&bar[q % PL_STAGES], (q / PL_STAGES) & 1);
     }
 }
 
@@ -668,7 +668,7 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
         float* out = (s & 1) ? Ca : Cb;
         const int full = (full_first && s < 2) ? 1 : 0;
         if (tma)
-            k_plume_step_tma<<<tgrid, dim3(TZ, TY), 0, st>>>((s & 1) ? map_b : map_a, out, mask, p->nx, p->ny, p->nz,
+            k_plume_step_tma<<<tgrid, dim3(TZ, PL_TY), 0, st>>>((s & 1) ? map_b : map_a, out, mask, p->nx, p->ny, p->nz,
                                                              xc, c, full ? nullptr : zlimit, full, err);
         else
             k_plume_step<<<grid, dim3(TZ, TY), 0, st>>>(p->nx, p->ny, p->nz, c, in, out, mask,
