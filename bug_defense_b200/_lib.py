@@ -161,6 +161,7 @@ class RecordHead(Structure):
 TUNE_MC_BLOCKS_PER_SM = 0
 TUNE_STENCIL_XC = 1
 TUNE_PLUME_XC = 2
+TUNE_PLUME_KERNEL = 3
 
 CONV_FWD_RELU = 0
 CONV_FWD_UPADD = 1

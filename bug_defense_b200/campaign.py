@@ -150,17 +150,18 @@ def _stage_ms(eng, n_epochs: int, laser: bool) -> np.ndarray:
 def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=None) -> dict:
     """Pick launch shapes by timing them on a throwaway engine of the real workload: `inst` is a
     campaign instance dict or a callable returning an engine with a `laser_power` attribute.
-    Tries MC CTAs per SM (photons per thread) on laser-on epochs and x-planes per CTA of the
-    fused substep and plume kernels; sets the winning values process-wide (bd_tune_set) and
+    Tries MC CTAs per SM (photons per thread) on laser-on epochs, x-planes per CTA of the fused
+    substep kernel, the plume kernel and its x-planes (kernel 0) or CTAs per SM (kernel 1); sets the winning values process-wide (bd_tune_set) and
     returns the choices with every trial's per-epoch stage time (ms)."""
     from . import _lib
     cand = dict(candidates or {})
     cand.setdefault(_lib.TUNE_MC_BLOCKS_PER_SM, [2, 4, 6, 8])
     cand.setdefault(_lib.TUNE_STENCIL_XC, [4, 8, 16])
+    cand.setdefault(_lib.TUNE_PLUME_KERNEL, [0, 1, 2])
     cand.setdefault(_lib.TUNE_PLUME_XC, [2, 4, 8])
-    stage = {_lib.TUNE_MC_BLOCKS_PER_SM: 0, _lib.TUNE_STENCIL_XC: 1, _lib.TUNE_PLUME_XC: 2}
+    stage = {_lib.TUNE_MC_BLOCKS_PER_SM: 0, _lib.TUNE_STENCIL_XC: 1, _lib.TUNE_PLUME_XC: 2, _lib.TUNE_PLUME_KERNEL: 2}
     names = {_lib.TUNE_MC_BLOCKS_PER_SM: "mc_ctas_per_sm", _lib.TUNE_STENCIL_XC: "stencil_xc",
-             _lib.TUNE_PLUME_XC: "plume_xc"}
+             _lib.TUNE_PLUME_XC: "plume_xc", _lib.TUNE_PLUME_KERNEL: "plume_kernel"}
     eng = inst() if callable(inst) else make_engine(inst, device=device)
     eng.step_epochs(3)                       # warm-up: graphs, caches, a first crater
     out = {"trials": {}}

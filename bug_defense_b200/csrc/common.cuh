@@ -22,6 +22,10 @@ int cuda_status(cudaError_t e, const char* what);
 // below 2^62.
 constexpr float kTallyScale = 68719476736.0f;          // 2^36
 constexpr long long kTallyMaxPhotons = 1LL << 26;
+// Plume neighbourhood mask: one byte per voxel, z rows padded to a 16-byte pitch (TMA rows).
+inline int plume_mask_pitch(int nz) { return (nz + 15) / 16 * 16; }
+inline size_t plume_mask_bytes(int nx, int ny, int nz) { return (size_t)nx * ny * plume_mask_pitch(nz); }
+
 // Launch-shape knobs (BD_TUNE_*) and the generation counter bumped by every change.
 int tune_value(int knob);
 int tune_generation();

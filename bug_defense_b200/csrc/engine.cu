@@ -209,7 +209,7 @@ extern "C" int bd_engine_create(const BdEngineDesc* desc, BdEngine** out) {
     for (int q = 0; q < 4 && err == cudaSuccess; ++q) err = cudaEventCreate(&e->ev[q]);
     if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->cap_stream, cudaStreamNonBlocking);
     if (err == cudaSuccess && desc->has_plume_transport)
-        err = cudaMalloc(&e->plume_mask, (size_t)desc->phase.nx * desc->phase.ny * desc->phase.nz);
+        err = cudaMalloc(&e->plume_mask, plume_mask_bytes(desc->phase.nx, desc->phase.ny, desc->phase.nz));
     if (err != cudaSuccess) {
         bd_engine_destroy(e);
         return cuda_status(err, "bd_engine_create");

@@ -281,14 +281,15 @@ struct PlumeConst {
     float vz_over_dz, dtp, decay;
 };
 
-// Plume neighbourhood byte per voxel, rebuilt whenever the void domain changes (epoch end):
+// Plume neighbourhood byte per voxel, rebuilt whenever the void domain changes (epoch end); the
+// bytes of one (x, y) column start every mz = plume_mask_pitch(nz) bytes (16-byte rows for TMA):
 //   bit 6: voxel is void            bit 7: voxel is void and not on an outer wall (FTCS update)
 //   bits 0-5: -x +x -y +y -z +z neighbour is void (otherwise its value is replaced by the centre,
 //   the zero-flux wall of plume.py:61-71)
 #define BD_PM_VOID 0x40u
 #define BD_PM_UPDATE 0x80u
-__global__ void k_plume_mask(int nx, int ny, int nz, const uint8_t* __restrict__ F, uint8_t* __restrict__ M,
-                             const int* __restrict__ zlimit) {
+__global__ void k_plume_mask(int nx, int ny, int nz, int mz, const uint8_t* __restrict__ F,
+                             uint8_t* __restrict__ M, const int* __restrict__ zlimit) {
     const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
     const int j = blockIdx.x * TY + threadIdx.y;
     const int i = blockIdx.y;
@@ -296,6 +297,7 @@ __global__ void k_plume_mask(int nx, int ny, int nz, const uint8_t* __restrict__
     const int plane = ny * nz;
     const bool xy_interior = (i > 0 && i < nx - 1 && j > 0 && j < ny - 1);
     const int col = i * plane + j * nz;
+    const size_t mcol = ((size_t)i * ny + j) * mz;
     for (int k = threadIdx.x; k < zl; k += TZ) {
         const int idx = col + k;
         uint8_t m = 0;
@@ -311,7 +313,7 @@ __global__ void k_plume_mask(int nx, int ny, int nz, const uint8_t* __restrict__
                 m |= (F[idx + 1] & BD_FLAG_VOID) ? 0x20 : 0;
             }
         }
-        M[idx] = m;
+        M[mcol + k] = m;
     }
 }
 
@@ -321,7 +323,7 @@ __global__ void k_plume_mask(int nx, int ny, int nz, const uint8_t* __restrict__
 // are loaded unconditionally and selected, so no load depends on another. Non-void voxels are
 // written (as 0) only when full_write is set: the engine keeps them 0 in both ping-pong
 // buffers, so a step touches only the void domain plus one mask byte per voxel.
-__global__ void __launch_bounds__(TZ * TY) k_plume_step(int nx, int ny, int nz, PlumeConst c,
+__global__ void __launch_bounds__(TZ * TY) k_plume_step(int nx, int ny, int nz, int mz, PlumeConst c,
                                                         const float* __restrict__ C, float* __restrict__ Cn,
                                                         const uint8_t* __restrict__ M,
                                                         const int* __restrict__ zlimit, int full_write) {
@@ -331,9 +333,10 @@ __global__ void __launch_bounds__(TZ * TY) k_plume_step(int nx, int ny, int nz, 
     if (j >= ny) return;
     const int plane = ny * nz;
     const int col = i * plane + j * nz;
+    const size_t mcol = ((size_t)i * ny + j) * mz;
     for (int k = threadIdx.x; k < zl; k += TZ) {
         const int idx = col + k;
-        const uint8_t m = __ldg(&M[idx]);
+        const uint8_t m = __ldg(&M[mcol + k]);
         if (!(m & BD_PM_UPDATE)) {
             if ((m & BD_PM_VOID) || full_write) Cn[idx] = 0.0f;
             continue;
@@ -373,7 +376,7 @@ static_assert(PL_STRIDE >= PL_PZ * PL_PY, "stage too small");
 
 __global__ void __launch_bounds__(TZ * PL_TY) k_plume_step_tma(const __grid_constant__ CUtensorMap in_map,
                                                                float* __restrict__ Cn, const uint8_t* __restrict__ M,
-                                                               int nx, int ny, int nz, int xc, PlumeConst c,
+                                                               int nx, int ny, int nz, int mz, int xc, PlumeConst c,
                                                                const int* __restrict__ zlimit, int full_write,
                                                                int* __restrict__ err) {
     __shared__ __align__(128) float ring[PL_STAGES][PL_STRIDE];
@@ -412,14 +415,15 @@ __global__ void __launch_bounds__(TZ * PL_TY) k_plume_step_tma(const __grid_cons
     for (int r = 0; r < PL_RY; ++r) {
         const int j = j0 + threadIdx.y + r * PL_TY;
         act[r] = kin && j < ny;
-        m[r] = act[r] ? __ldg(&M[ib * plane + j * nz + k]) : 0;   // next plane's bytes fetched a plane ahead
+        m[r] = act[r] ? __ldg(&M[((size_t)ib * ny + j) * mz + k]) : 0;   // next plane's bytes fetched a plane ahead
     }
     for (int i = ib; i < ie; ++i) {
         const int q = i - ib + 1;
         uint8_t nm[PL_RY];
 #pragma unroll
         for (int r = 0; r < PL_RY; ++r)
-            nm[r] = (act[r] && i + 1 < ie) ? __ldg(&M[(i + 1) * plane + (j0 + threadIdx.y + r * PL_TY) * nz + k]) : 0;
+            nm[r] = (act[r] && i + 1 < ie) ? __ldg(&M[((size_t)(i + 1) * ny + j0 + threadIdx.y + r * PL_TY) * mz + k])
+                                           : 0;
         if (tid == 0 && !s_fail && !mbar_wait(&bar[(q + 1) % PL_STAGES], ((q + 1) / PL_STAGES) & 1)) s_fail = 1;
         __syncthreads();  // load q+1 landed (seen by thread 0); every thread is done with plane i-2's stage
         if (tid == 0 && q + PL_STAGES - 2 < nplanes) {
@@ -458,6 +462,226 @@ __global__ void __launch_bounds__(TZ * PL_TY) k_plume_step_tma(const __grid_cons
         // drain: every copy issued gets a bounded chance to land before the CTA exits
         const int last = min(nplanes, nplanes - 2 + PL_STAGES - 1);
         for (int q = max(0, last - PL_STAGES); q < last; ++q) mbar_wait(&bar[q % PL_STAGES], (q / PL_STAGES) & 1);
+    }
+}
+
+// Persistent x-marching plume step. A tile is 32 (z) x 32 (y) voxels and a CTA has 8 consumer
+// warps, one per 4-voxel z group; lane l of a warp owns row l of the tile, so a thread holds one
+// float4 (4 consecutive z voxels) and a warp's 32 rows share their z range: whether its voxels
+// are tissue, bulk void or void next to a wall is (almost always) uniform over the warp. Three
+// warp-uniform paths follow: no void voxel (nothing to do), every voxel updated with all six
+// neighbours void (the FTCS expression with no selects), and the general path with the
+// zero-flux neighbour selects. All three evaluate the same expression per voxel, so the result
+// is bit-identical to the scalar kernel. A thread marches its row along x keeping the x-1 / x /
+// x+1 float4 in registers; the y and z neighbours and the mask bytes come from the centre plane.
+// The work is the columns (z tile, y tile) above the void limit times their nx planes, laid end
+// to end and cut into gridDim.x equal runs (one or two column segments per CTA, the x halo paid
+// once per segment). A producer warp streams each segment's planes ib-1 .. ie, PB planes per
+// copy (the concentration planes with a 1-voxel y and 4 / 8-voxel z halo, 44 floats wide so that
+// the 32 rows a warp reads fall in distinct banks, plus the planes' 32 x 32 mask bytes, on one
+// mbarrier) through a PX_STAGES ring; consumer warps wait on a stage's full barrier and release
+// it on its empty barrier once its last plane has been a centre. An mbarrier round trip costs a
+// few hundred cycles, comparable to the arithmetic of one 32 x 32 plane, hence several planes
+// per stage. Needs nz % 4 == 0. A store writes the whole float4 when all four voxels are void
+// (or full_write), else only the void ones.
+constexpr int PX_STAGES = 4;  // power of two
+constexpr int PX_NW = 8, PX_THREADS = 32 * (PX_NW + 1);
+constexpr int PX_PZ = 44, PX_BY = 32, PX_PY = PX_BY + 2;
+constexpr unsigned PX_PLANE = PX_PZ * PX_PY * sizeof(float);  // one concentration plane of a stage
+constexpr unsigned PX_MPLANE = PL_BZ * PX_BY;                  // one mask plane
+static_assert(PX_PZ % 4 == 0 && PX_PZ >= PL_BZ + 5, "z box must hold the tile, both z neighbours, 16-byte rows");
+static_assert(PX_PLANE % 16 == 0 && PX_MPLANE % 16 == 0, "planes must keep 16-byte alignment");
+template <int PB>
+struct PlumeXM {
+    static constexpr unsigned C_BYTES = PB * PX_PLANE;
+    static constexpr unsigned M_OFF = (C_BYTES + 127) / 128 * 128;
+    static constexpr unsigned M_BYTES = PB * PX_MPLANE;
+    static constexpr unsigned STAGE = (M_OFF + M_BYTES + 127) / 128 * 128;
+    static constexpr unsigned SMEM = PX_STAGES * STAGE;  // dynamic shared memory per CTA
+};
+
+// A CTA's run of planes [s0, s1) over the columns laid end to end (column = z tile fastest, then
+// y tile; nx planes each), walked as segments (k0, j0, ib, ie) that each stay in one column.
+struct PlumeRun {
+    int n_kt, nx;
+    long long s0, s1;
+    __device__ __forceinline__ int4 segment(long long pos) const {
+        const int col = (int)(pos / nx), ib = (int)(pos - (long long)col * nx);
+        const int ie = (int)min((long long)nx, ib + (s1 - pos));
+        return make_int4((col % n_kt) * PL_BZ, (col / n_kt) * PX_BY, ib, ie);
+    }
+};
+
+// Every lane waits for the copy of load q; the vote keeps a timeout warp-uniform.
+__device__ __forceinline__ bool px_wait(unsigned long long* full, int q, volatile int* fail) {
+    const bool good = !*fail && mbar_wait(&full[q & (PX_STAGES - 1)], (q / PX_STAGES) & 1);
+    if (__all_sync(0xffffffffu, good)) return true;
+    *fail = 1;
+    return false;
+}
+
+// Every lane is done reading stage q: release it (one arrival per consumer warp).
+__device__ __forceinline__ void px_release(unsigned long long* empty, int q, int lane) {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[q & (PX_STAGES - 1)]);
+}
+
+template <int PB>
+__global__ void __launch_bounds__(PX_THREADS, 1) k_plume_xm(const __grid_constant__ CUtensorMap c_map,
+                                                         const __grid_constant__ CUtensorMap m_map,
+                                                         float* __restrict__ Cn, int nx, int ny, int nz, PlumeConst c,
+                                                         const int* __restrict__ zlimit, int full_write,
+                                                         int* __restrict__ err) {
+    using X = PlumeXM<PB>;
+    extern __shared__ __align__(128) unsigned char ring[];
+    __shared__ __align__(8) unsigned long long full[PX_STAGES], empty[PX_STAGES];
+    __shared__ volatile int s_fail;
+    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
+    const int n_kt = (zl + PL_BZ - 1) / PL_BZ;
+    const long long total = (long long)n_kt * ((ny + PX_BY - 1) / PX_BY) * nx;
+    const PlumeRun run{n_kt, nx, total * blockIdx.x / gridDim.x, total * (blockIdx.x + 1) / gridDim.x};
+    if (run.s0 >= run.s1) return;  // uniform over the CTA
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        for (int q = 0; q < PX_STAGES; ++q) {
+            mbar_init(&full[q], 1);
+            mbar_init(&empty[q], PX_NW);
+        }
+        mbar_init_fence();
+        s_fail = 0;
+    }
+    __syncthreads();
+    int issued = 0;  // producer: loads issued
+    if (warp == PX_NW) {
+        // ---- producer warp (one lane): planes ib-1 .. ie of each segment, PB per load ----
+        if (lane == 0) {
+            for (long long pos = run.s0; pos < run.s1 && !s_fail;) {
+                const int4 t = run.segment(pos);
+                pos += t.w - t.z;
+                const int nb = (t.w - t.z + 2 + PB - 1) / PB;
+                for (int b = 0; b < nb; ++b) {
+                    const int sl = issued & (PX_STAGES - 1);
+                    if (issued >= PX_STAGES && !mbar_wait(&empty[sl], ((issued / PX_STAGES) - 1) & 1)) {
+                        s_fail = 1;
+                        break;
+                    }
+                    mbar_expect_tx(&full[sl], X::C_BYTES + X::M_BYTES);
+                    unsigned char* st = ring + sl * X::STAGE;
+                    tma_load_3d(st, &c_map, t.x - 4, t.y - 1, t.z - 1 + PB * b, &full[sl]);
+                    tma_load_3d(st + X::M_OFF, &m_map, t.x, t.y, t.z - 1 + PB * b, &full[sl]);
+                    ++issued;
+                }
+            }
+        }
+    } else {
+        // ---- consumer warps: warp = z group, lane = tile row ----
+        const float wx = c.dtp * c.dxy_x, wy = c.dtp * c.dxy_y, wb = c.dtp * c.dz_z;
+        const float wt = wb + c.dtp * c.vz_over_dz;
+        const float w0 = 1.0f - 2.0f * (wx + wy + wb) - c.dtp * c.vz_over_dz;
+        const int plane = ny * nz;
+        const int t0 = (lane + 1) * PX_PZ + 4 + 4 * warp;  // this thread's float4 in a plane (16-byte aligned)
+        const int mo = X::M_OFF + lane * PL_BZ + 4 * warp;  // its four mask bytes in mask plane 0
+        int L = 0;                                          // load index of the segment's first load
+        bool ok = true;
+        for (long long pos = run.s0; pos < run.s1 && ok;) {
+            const int4 t = run.segment(pos);
+            const int k0 = t.x, j0 = t.y, ib = t.z, ie = t.w;
+            pos += ie - ib;
+            const int np = ie - ib + 2, nb = (np + PB - 1) / PB;  // planes ib-1 .. ie in nb loads
+            const int k = k0 + 4 * warp;
+            // bytes of voxels at or below zl are cleared: the mask is only rebuilt above zl
+            const int nk = zl - k;
+            const unsigned zkeep = nk >= 4 ? 0xffffffffu : (nk <= 0 ? 0u : (0xffffffffu >> (8 * (4 - nk))));
+            const bool act = nk > 0 && j0 + lane < ny;
+            float* dst = Cn + (size_t)ib * plane + (size_t)(j0 + lane) * nz + k;
+            int waited = 0, released = 0;  // loads of this segment waited for / released
+            // segment plane q lives in load q / PB, plane q % PB of that stage
+#define BD_PX_PLANE(q) (ring + ((L + (q) / PB) & (PX_STAGES - 1)) * X::STAGE + ((q) % PB) * PX_PLANE)
+#define BD_PX_NEED(q)                                                         \
+    while (ok && waited <= (q) / PB) {                                        \
+        if (!px_wait(full, L + waited, &s_fail)) ok = false;                  \
+        ++waited;                                                             \
+    }
+            BD_PX_NEED(1)
+            if (!ok) break;
+            float4 cw = *reinterpret_cast<const float4*>(BD_PX_PLANE(0) + 4 * t0);
+            float4 cc = *reinterpret_cast<const float4*>(BD_PX_PLANE(1) + 4 * t0);
+            if (PB == 1) { px_release(empty, L, lane); released = 1; }
+            for (int q = 1; q < np - 1; ++q, dst += plane) {  // q: centre plane (x = ib - 1 + q)
+                BD_PX_NEED(q + 1)
+                if (!ok) break;
+                const unsigned char* sc = BD_PX_PLANE(q);
+                const float* tc = reinterpret_cast<const float*>(sc);
+                const float4 ce = *reinterpret_cast<const float4*>(BD_PX_PLANE(q + 1) + 4 * t0);
+                const unsigned mr =
+                    *reinterpret_cast<const unsigned*>(ring + ((L + q / PB) & (PX_STAGES - 1)) * X::STAGE + mo +
+                                                       (q % PB) * PX_MPLANE) & zkeep;
+                const unsigned vd = mr & 0x40404040u;  // void bit of each of the four voxels
+                const bool bulk = (mr & 0xBFBFBFBFu) == 0xBFBFBFBFu;  // all updated, all neighbours void
+                if (__any_sync(0xffffffffu, act && (vd || full_write))) {
+                    const float4 cs = *reinterpret_cast<const float4*>(tc + t0 - PX_PZ);
+                    const float4 cn = *reinterpret_cast<const float4*>(tc + t0 + PX_PZ);
+                    const float zb = tc[t0 - 1], zt = tc[t0 + 4];
+                    float v[4];
+                    if (__all_sync(0xffffffffu, bulk || !act)) {
+                        v[0] = fmaxf((w0 * cc.x + wx * (cw.x + ce.x) + wy * (cs.x + cn.x) + wb * zb + wt * cc.y) * c.decay, 0.0f);
+                        v[1] = fmaxf((w0 * cc.y + wx * (cw.y + ce.y) + wy * (cs.y + cn.y) + wb * cc.x + wt * cc.z) * c.decay, 0.0f);
+                        v[2] = fmaxf((w0 * cc.z + wx * (cw.z + ce.z) + wy * (cs.z + cn.z) + wb * cc.y + wt * cc.w) * c.decay, 0.0f);
+                        v[3] = fmaxf((w0 * cc.w + wx * (cw.w + ce.w) + wy * (cs.w + cn.w) + wb * cc.z + wt * zt) * c.decay, 0.0f);
+                    } else {
+                        const float c0v[4] = {cc.x, cc.y, cc.z, cc.w};
+                        const float cwv[4] = {cw.x, cw.y, cw.z, cw.w};
+                        const float cev[4] = {ce.x, ce.y, ce.z, ce.w};
+                        const float csv[4] = {cs.x, cs.y, cs.z, cs.w};
+                        const float cnv[4] = {cn.x, cn.y, cn.z, cn.w};
+                        const float cbv[4] = {zb, cc.x, cc.y, cc.z};
+                        const float ctv[4] = {cc.y, cc.z, cc.w, zt};
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) {
+                            const unsigned me = mr >> (8 * e);
+                            const float c0 = c0v[e];
+                            const float w = (me & 0x01) ? cwv[e] : c0;
+                            const float ee = (me & 0x02) ? cev[e] : c0;
+                            const float sx = (me & 0x04) ? csv[e] : c0;
+                            const float nn = (me & 0x08) ? cnv[e] : c0;
+                            const float b = (me & 0x10) ? cbv[e] : c0;
+                            const float tz = (me & 0x20) ? ctv[e] : c0;
+                            const float u =
+                                fmaxf((w0 * c0 + wx * (w + ee) + wy * (sx + nn) + wb * b + wt * tz) * c.decay, 0.0f);
+                            v[e] = (me & BD_PM_UPDATE) ? u : 0.0f;
+                        }
+                    }
+                    if (act && (vd || full_write)) {
+                        if (full_write || vd == 0x40404040u) {
+                            *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+                        } else {
+#pragma unroll
+                            for (int e = 0; e < 4; ++e)
+                                if (vd & (0x40u << (8 * e))) dst[e] = v[e];
+                        }
+                    }
+                }
+                // plane q was the last plane of its load: every plane of that load has been read
+                if ((q + 1) % PB == 0) {
+                    px_release(empty, L + released, lane);
+                    ++released;
+                }
+                cw = cc;
+                cc = ce;
+            }
+            if (!ok) break;
+            for (; released < nb; ++released) px_release(empty, L + released, lane);
+            L += nb;
+#undef BD_PX_PLANE
+#undef BD_PX_NEED
+        }
+    }
+    __syncthreads();
+    if (tid == PX_NW * 32 && s_fail) {
+        atomicExch(err, 1);
+        // drain: the copies still in flight get a bounded chance to land before the CTA exits
+        for (int q = max(0, issued - PX_STAGES); q < issued; ++q)
+            mbar_wait(&full[q & (PX_STAGES - 1)], (q / PX_STAGES) & 1);
     }
 }
 
@@ -651,27 +875,60 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     c.dtp = dtp;
     c.decay = decay;
     const dim3 grid((p->ny + TY - 1) / TY, p->nx);
+    const int mz = plume_mask_pitch(p->nz);
     // with full_first the whole grid is masked (the context API's first steps write every voxel)
-    k_plume_mask<<<grid, dim3(TZ, TY), 0, st>>>(p->nx, p->ny, p->nz, F, mask, full_first ? nullptr : zlimit);
+    k_plume_mask<<<grid, dim3(TZ, TY), 0, st>>>(p->nx, p->ny, p->nz, mz, F, mask, full_first ? nullptr : zlimit);
     BD_CHECK_LAUNCH("k_plume_mask");
-    CUtensorMap map_a, map_b;
+    CUtensorMap map_a, map_b, map_m;
 #ifdef BD_NO_TMA
     err = nullptr;
 #endif
-    const bool tma = err != nullptr && make_tmap_3d_f32(&map_a, Ca, p->nx, p->ny, p->nz, PL_PZ, PL_PY, 1) &&
-                     make_tmap_3d_f32(&map_b, Cb, p->nx, p->ny, p->nz, PL_PZ, PL_PY, 1);
+    // plume kernel: 0 = scalar TMA kernel, 1 / 2 = persistent x-marching kernel, 2 / 4 planes per copy
+    // (one CTA per SM register budget: 64 registers x 288 threads, so at most 3 CTAs per SM)
+    const int shape = tune_value(BD_TUNE_PLUME_KERNEL);
+    const int pb = shape == 1 ? 2 : 4;
+    const int py = shape == 0 ? PL_PY : PX_PY;
+    const int pz = shape == 0 ? PL_PZ : PX_PZ;
+    const int bx = shape == 0 ? 1 : pb;
+    const bool tma = err != nullptr && make_tmap_3d_f32(&map_a, Ca, p->nx, p->ny, p->nz, pz, py, bx) &&
+                     make_tmap_3d_f32(&map_b, Cb, p->nx, p->ny, p->nz, pz, py, bx) &&
+                     (shape == 0 || make_tmap_3d_u8(&map_m, mask, p->nx, p->ny, p->nz, mz, PL_BZ, PX_BY, pb));
     const int xc = tune_value(BD_TUNE_PLUME_XC);
     const dim3 tgrid((p->nz + PL_BZ - 1) / PL_BZ, (p->ny + PL_BY - 1) / PL_BY, (p->nx + xc - 1) / xc);
+    // persistent kernel: xc CTAs per SM (capped by occupancy), at most one per plane of the grid
+    int xm_grid = 0;
+    unsigned xm_smem = shape == 1 ? PlumeXM<2>::SMEM : PlumeXM<4>::SMEM;
+    if (tma && shape > 0) {
+        int dev = 0, sms = 0, occ = 0;
+        BD_CUDA(cudaGetDevice(&dev));
+        BD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        if (shape == 1) {
+            BD_CUDA(cudaFuncSetAttribute(k_plume_xm<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, xm_smem));
+            BD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_plume_xm<2>, PX_THREADS, xm_smem));
+        } else {
+            BD_CUDA(cudaFuncSetAttribute(k_plume_xm<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, xm_smem));
+            BD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_plume_xm<4>, PX_THREADS, xm_smem));
+        }
+        const long long planes =
+            (long long)((p->nz + PL_BZ - 1) / PL_BZ) * ((p->ny + PX_BY - 1) / PX_BY) * p->nx;
+        xm_grid = (int)std::max(1LL, std::min(planes, (long long)std::max(std::min(occ, xc), 1) * sms));
+    }
     const long long total = (long long)steps * n_substeps;
     for (long long s = 0; s < total; ++s) {
         const float* in = (s & 1) ? Cb : Ca;
         float* out = (s & 1) ? Ca : Cb;
         const int full = (full_first && s < 2) ? 1 : 0;
-        if (tma)
-            k_plume_step_tma<<<tgrid, dim3(TZ, PL_TY), 0, st>>>((s & 1) ? map_b : map_a, out, mask, p->nx, p->ny, p->nz,
-                                                             xc, c, full ? nullptr : zlimit, full, err);
+        const CUtensorMap& map = (s & 1) ? map_b : map_a;
+        const int* zl = full ? nullptr : zlimit;
+        if (tma && shape == 1)
+            k_plume_xm<2><<<xm_grid, PX_THREADS, xm_smem, st>>>(map, map_m, out, p->nx, p->ny, p->nz, c, zl, full, err);
+        else if (tma && shape == 2)
+            k_plume_xm<4><<<xm_grid, PX_THREADS, xm_smem, st>>>(map, map_m, out, p->nx, p->ny, p->nz, c, zl, full, err);
+        else if (tma)
+            k_plume_step_tma<<<tgrid, dim3(TZ, PL_TY), 0, st>>>(map, out, mask, p->nx, p->ny, p->nz, mz, xc, c, zl,
+                                                             full, err);
         else
-            k_plume_step<<<grid, dim3(TZ, TY), 0, st>>>(p->nx, p->ny, p->nz, c, in, out, mask,
+            k_plume_step<<<grid, dim3(TZ, TY), 0, st>>>(p->nx, p->ny, p->nz, mz, c, in, out, mask,
                                                         full ? nullptr : zlimit, full);
     }
     BD_CHECK_LAUNCH("k_plume_step");
@@ -710,9 +967,8 @@ extern "C" int bd_plume_advance(const BdPlumeParams* p, float* Ca, float* Cb, in
         return BD_OK;
     }
     cudaStream_t st = as_stream(stream);
-    const size_t nv = (size_t)p->nx * p->ny * p->nz;
     unsigned char* scratch = nullptr;  // plume neighbourhood bytes + a 4-byte error flag
-    const size_t flag_off = (nv + 15) & ~(size_t)15;
+    const size_t flag_off = plume_mask_bytes(p->nx, p->ny, p->nz);
     BD_CUDA(cudaMallocAsync((void**)&scratch, flag_off + 16, st));
     int* err = reinterpret_cast<int*>(scratch + flag_off);
     int rc = BD_OK;

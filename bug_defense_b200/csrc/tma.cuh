@@ -17,6 +17,9 @@ constexpr unsigned TMA_SUSPEND_NS = 1000;
 // 3-D tiled map over a float grid: dims (innermost first) {nz, ny, nx}; box {bz, by, bx}.
 // Requires nz % 4 == 0 (16-byte row stride) and a 16-byte aligned base; returns false otherwise.
 bool make_tmap_3d_f32(CUtensorMap* out, const void* base, int nx, int ny, int nz, int bz, int by, int bx);
+// 3-D tiled map over a byte grid whose z rows are `pitch` bytes apart (pitch % 16 == 0, >= nz);
+// elements past nz read as 0.
+bool make_tmap_3d_u8(CUtensorMap* out, const void* base, int nx, int ny, int nz, int pitch, int bz, int by, int bx);
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -33,6 +36,11 @@ __device__ __forceinline__ void mbar_init_fence() {
 __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
                  : "memory");
+}
+
+// Plain arrive (count 1) on an mbarrier; release semantics order this thread's earlier accesses.
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
 // Bounded wait for the phase with the given parity; returns false on timeout.

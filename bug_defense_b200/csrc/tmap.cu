@@ -40,4 +40,18 @@ bool make_tmap_3d_f32(CUtensorMap* out, const void* base, int nx, int ny, int nz
     return r == CUDA_SUCCESS;
 }
 
+bool make_tmap_3d_u8(CUtensorMap* out, const void* base, int nx, int ny, int nz, int pitch, int bz, int by, int bx) {
+    if (pitch % 16 != 0 || pitch < nz || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)nz, (cuuint64_t)ny, (cuuint64_t)nx};
+    cuuint64_t strides[2] = {(cuuint64_t)pitch, (cuuint64_t)ny * pitch};
+    cuuint32_t box[3] = {(cuuint32_t)bz, (cuuint32_t)by, (cuuint32_t)bx};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(out, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 }  // namespace bd

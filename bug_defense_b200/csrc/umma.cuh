@@ -96,9 +96,5 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
         : "memory");
 }
 
-// Plain arrive (count 1) on an mbarrier.
-__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
 
 }  // namespace bd

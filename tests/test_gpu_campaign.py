@@ -21,7 +21,8 @@ def _knob(k, v=None):
 @pytest.fixture
 def restore_knobs(gpu):
     from bug_defense_b200 import _lib
-    keep = {k: _knob(k) for k in (_lib.TUNE_MC_BLOCKS_PER_SM, _lib.TUNE_STENCIL_XC, _lib.TUNE_PLUME_XC)}
+    keep = {k: _knob(k) for k in (_lib.TUNE_MC_BLOCKS_PER_SM, _lib.TUNE_STENCIL_XC, _lib.TUNE_PLUME_XC,
+                                  _lib.TUNE_PLUME_KERNEL)}
     yield
     for k, v in keep.items():
         _knob(k, v)
@@ -33,6 +34,8 @@ def test_knob_validation(gpu, restore_knobs):
         _knob(_lib.TUNE_STENCIL_XC, 0)
     with pytest.raises(ValueError):
         _knob(_lib.TUNE_MC_BLOCKS_PER_SM, 17)
+    with pytest.raises(ValueError):
+        _knob(_lib.TUNE_PLUME_KERNEL, 3)
     with pytest.raises(ValueError):
         _knob(7, 1)
 
@@ -57,6 +60,48 @@ def test_launch_shapes_leave_results_bit_identical(gpu, restore_knobs):
         _knob(_lib.TUNE_MC_BLOCKS_PER_SM, blocks)
         maps.append(gpu.run_voxel_mc3d(**kw)["A_3d"])
     assert np.array_equal(maps[0], maps[1]) and np.array_equal(maps[0], maps[2])
+
+
+def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
+    """The scalar plume kernel (several x-chunk lengths) and the persistent x-marching kernel
+    (several grid sizes, i.e. run splits) give the same bits: through the context API (full writes
+    on the first steps, ragged y tiles, scattered void) and through the engine (void z-limit,
+    partly void 4-voxel groups at the crater walls, bulk-void fast path)."""
+    from bug_defense_b200 import _lib, campaign
+    rng = np.random.default_rng(11)
+    scattered = rng.uniform(size=(9, 35, 68)) < 0.7
+    slab = np.zeros((12, 70, 96), bool)                 # bulk void above z = 50, scattered pores below
+    slab[:, :, :50] = True
+    slab |= rng.uniform(size=slab.shape) < 0.1
+    for vd in (scattered, slab):
+        shape = vd.shape
+        C0 = (rng.uniform(0, 1, shape) * vd).astype(np.float32)
+        z = np.zeros(shape)
+        fields = []
+        for kern, xc in ((0, 4), (0, 2), (1, 4), (1, 1), (2, 2), (2, 1), (1, 3)):
+            _knob(_lib.TUNE_PLUME_KERNEL, kern)
+            _knob(_lib.TUNE_PLUME_XC, xc)
+            ctx = gpu.MetalAblationContext(*shape, 0.03, 0.025, 0.02, 1e-5, 0.0, 20.0, 100.0, 300.0,
+                                           plume_params={'D_xy': 1.5, 'D_z': 2.5, 'vz': 4.0, 'tau_linger': 0.02},
+                                           plume_dt_policy='as_given')
+            ctx.set_state(np.full(shape, 20.0), z, z, z, np.zeros(shape, np.uint8), np.zeros(shape, np.uint8), z,
+                          z, np.full(shape, 1e-3), plume=C0, plume_void=vd)
+            ctx.advance_substeps(7, is_active=0)
+            fields.append(ctx.get_plume())
+        for f in fields[1:]:
+            assert np.array_equal(f, fields[0])
+        assert np.any(fields[0] != C0)
+    inst = _small(22)                                  # 2940 nm, 80 W: a crater opens
+    runs = []
+    for kern in (0, 1, 2):
+        _knob(_lib.TUNE_PLUME_KERNEL, kern)
+        camp = campaign.Campaign([inst])
+        camp.run(14, sync_every=14)
+        e = camp.engines[0]
+        runs.append((e.T.copy(), e.plume.raw.double().cpu().numpy(), e.ablated.copy()))
+    assert runs[0][2].sum() > 0 and np.any(runs[0][1] > 0)
+    for r in runs[1:]:
+        assert all(np.array_equal(a, b) for a, b in zip(r, runs[0]))
 
 
 def _small(index, photons=20_000):
@@ -86,9 +131,9 @@ def test_autotune_sets_the_fastest_candidates(gpu, restore_knobs):
     from bug_defense_b200 import _lib, campaign
     res = campaign.autotune(_small(4), epochs_per_trial=2,
                             candidates={_lib.TUNE_MC_BLOCKS_PER_SM: [2, 4], _lib.TUNE_STENCIL_XC: [4, 8],
-                                        _lib.TUNE_PLUME_XC: [2, 4]})
+                                        _lib.TUNE_PLUME_KERNEL: [0, 2], _lib.TUNE_PLUME_XC: [2, 4]})
     for name, knob in (("mc_ctas_per_sm", _lib.TUNE_MC_BLOCKS_PER_SM), ("stencil_xc", _lib.TUNE_STENCIL_XC),
-                       ("plume_xc", _lib.TUNE_PLUME_XC)):
+                       ("plume_kernel", _lib.TUNE_PLUME_KERNEL), ("plume_xc", _lib.TUNE_PLUME_XC)):
         trials = res["trials"][name]
         assert [v for v, _ in trials] == sorted(v for v, _ in trials) and all(t > 0 for _, t in trials)
         assert res[name] == min(trials, key=lambda t: t[1])[0] == _knob(knob)
