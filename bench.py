@@ -287,10 +287,14 @@ def ours_main(args):
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
         tj = json.loads(tf.read_text())
-        key = {"substeps": "k_substep", "plume": "k_plume_step"}[dom]
+        key = {"substeps": "k_substep", "plume": plume_kernel.split("<")[0]}[dom]
         if key in tj:
             traffic = tj[key]["bytes_per_voxel"] * eng.Nx * eng.Ny * eng.Nz
-    roof = {"bound": "hbm", "kernel": {"substeps": "k_substep<fused ablation>", "plume": "k_plume_step"}[dom],
+    from bug_defense_b200 import _lib
+    kv = ctypes.c_int(0)
+    _lib.call("bd_tune_get", _lib.TUNE_PLUME_KERNEL, ctypes.byref(kv))
+    plume_kernel = {0: "k_plume_step_tma", 1: "k_plume_xm<2>", 2: "k_plume_xm<4>"}.get(kv.value, "k_plume_step")
+    roof = {"bound": "hbm", "kernel": {"substeps": "k_substep<fused ablation>", "plume": plume_kernel}[dom],
             "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
             "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
             else "fallback 6650 GB/s", "algorithmic_bytes_per_launch": bytes_per_launch,
