@@ -469,9 +469,9 @@ __global__ void __launch_bounds__(TZ * PL_TY) k_plume_step_tma(const __grid_cons
 // warps, one per 4-voxel z group; lane l of a warp owns row l of the tile, so a thread holds one
 // float4 (4 consecutive z voxels) and a warp's 32 rows share their z range: whether its voxels
 // are tissue, bulk void or void next to a wall is (almost always) uniform over the warp. Three
-// warp-uniform paths follow: no void voxel (nothing to do), every voxel updated with all six
-// neighbours void (the FTCS expression with no selects), and the general path with the
-// zero-flux neighbour selects. All three evaluate the same expression per voxel, so the result
+// warp-uniform paths follow: no void voxel (nothing to do), every updated voxel with all six
+// neighbours void (the FTCS expression with no neighbour selects; outer-wall voxels, void but not
+// updated, take 0), and the general path with the zero-flux neighbour selects. All three evaluate the same expression per voxel, so the result
 // is bit-identical to the scalar kernel. A thread marches its row along x keeping the x-1 / x /
 // x+1 float4 in registers; the y and z neighbours and the mask bytes come from the centre plane.
 // The work is the columns (z tile, y tile) above the void limit times their nx planes, laid end
@@ -617,7 +617,10 @@ __global__ void __launch_bounds__(PX_THREADS, 1) k_plume_xm(const __grid_constan
                     *reinterpret_cast<const unsigned*>(ring + ((L + q / PB) & (PX_STAGES - 1)) * X::STAGE + mo +
                                                        (q % PB) * PX_MPLANE) & zkeep;
                 const unsigned vd = mr & 0x40404040u;  // void bit of each of the four voxels
-                const bool bulk = (mr & 0xBFBFBFBFu) == 0xBFBFBFBFu;  // all updated, all neighbours void
+                // every voxel that is updated has all six neighbours void (outer-wall and tissue voxels,
+                // not updated, take 0 as on the general path)
+                const unsigned upd = (mr >> 7) & 0x01010101u;
+                const bool bulk = (mr & (upd * 0x3Fu)) == upd * 0x3Fu;
                 if (__any_sync(0xffffffffu, act && (vd || full_write))) {
                     const float4 cs = *reinterpret_cast<const float4*>(tc + t0 - PX_PZ);
                     const float4 cn = *reinterpret_cast<const float4*>(tc + t0 + PX_PZ);
@@ -628,6 +631,8 @@ __global__ void __launch_bounds__(PX_THREADS, 1) k_plume_xm(const __grid_constan
                         v[1] = fmaxf((w0 * cc.y + wx * (cw.y + ce.y) + wy * (cs.y + cn.y) + wb * cc.x + wt * cc.z) * c.decay, 0.0f);
                         v[2] = fmaxf((w0 * cc.z + wx * (cw.z + ce.z) + wy * (cs.z + cn.z) + wb * cc.y + wt * cc.w) * c.decay, 0.0f);
                         v[3] = fmaxf((w0 * cc.w + wx * (cw.w + ce.w) + wy * (cs.w + cn.w) + wb * cc.z + wt * zt) * c.decay, 0.0f);
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) v[e] = ((upd >> (8 * e)) & 1u) ? v[e] : 0.0f;
                     } else {
                         const float c0v[4] = {cc.x, cc.y, cc.z, cc.w};
                         const float cwv[4] = {cw.x, cw.y, cw.z, cw.w};
