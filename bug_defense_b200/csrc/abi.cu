@@ -47,7 +47,7 @@ extern "C" int bd_tune_set(int knob, int value) {
     if (knob == BD_TUNE_MC_BLOCKS_PER_SM)
         BD_REQUIRE(value >= 0 && value <= 16, "bd_tune_set: MC CTAs per SM must be 0..16, got %d", value);
     else if (knob == BD_TUNE_PLUME_KERNEL)
-        BD_REQUIRE(value >= 0 && value <= 2, "bd_tune_set: plume kernel must be 0..2, got %d", value);
+        BD_REQUIRE(value >= 0 && value <= 3, "bd_tune_set: plume kernel must be 0..3, got %d", value);
     else
         BD_REQUIRE(value >= 1 && value <= 64, "bd_tune_set: x-planes per CTA must be 1..64, got %d", value);
     if (g_tune[knob].exchange(value) != value) g_tune_gen.fetch_add(1);

@@ -503,12 +503,12 @@ struct PlumeXM {
 // A CTA's run of planes [s0, s1) over the columns laid end to end (column = z tile fastest, then
 // y tile; nx planes each), walked as segments (k0, j0, ib, ie) that each stay in one column.
 struct PlumeRun {
-    int n_kt, nx;
+    int n_kt, by, nx;  // z tiles, y stride of the tiles, x planes per column
     long long s0, s1;
     __device__ __forceinline__ int4 segment(long long pos) const {
         const int col = (int)(pos / nx), ib = (int)(pos - (long long)col * nx);
         const int ie = (int)min((long long)nx, ib + (s1 - pos));
-        return make_int4((col % n_kt) * PL_BZ, (col / n_kt) * PX_BY, ib, ie);
+        return make_int4((col % n_kt) * PL_BZ, (col / n_kt) * by, ib, ie);
     }
 };
 
@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(PX_THREADS, 1) k_plume_xm(const __grid_constan
     const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
     const int n_kt = (zl + PL_BZ - 1) / PL_BZ;
     const long long total = (long long)n_kt * ((ny + PX_BY - 1) / PX_BY) * nx;
-    const PlumeRun run{n_kt, nx, total * blockIdx.x / gridDim.x, total * (blockIdx.x + 1) / gridDim.x};
+    const PlumeRun run{n_kt, PX_BY, nx, total * blockIdx.x / gridDim.x, total * (blockIdx.x + 1) / gridDim.x};
     if (run.s0 >= run.s1) return;  // uniform over the CTA
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
@@ -685,6 +685,240 @@ __global__ void __launch_bounds__(PX_THREADS, 1) k_plume_xm(const __grid_constan
     if (tid == PX_NW * 32 && s_fail) {
         atomicExch(err, 1);
         // drain: the copies still in flight get a bounded chance to land before the CTA exits
+        for (int q = max(0, issued - PX_STAGES); q < issued; ++q)
+            mbar_wait(&full[q & (PX_STAGES - 1)], (q / PX_STAGES) & 1);
+    }
+}
+
+// Two FTCS steps per pass (temporal blocking), otherwise the x-marching kernel's structure: the
+// plane stream, ring protocol, warp = 4-voxel z group and lane = row. Lane l holds row y = j0 - 1 + l;
+// each thread computes the first step on the 6 voxels z = k-1 .. k+4 of its row (its 4 plus both z
+// neighbours), the second step on its 4, taking the first step's y neighbours from lanes l +- 1 by
+// shuffle. Lanes 0 and 31 carry the first step's y halo, so a tile outputs 30 rows (j0 .. j0+29) and
+// a segment streams planes ib-2 .. ie+1. Per time step this halves the planes streamed, the ring
+// round trips, the global stores and the launches; the first step's values never leave registers.
+// Each voxel's update is the single-step expression (bit-identical to one-step kernels). The mask
+// tile is 64 bytes wide (z k0-16 .. k0+47) so the neighbours' bytes at k0-1 and k0+32 are present.
+// With full_write the result buffer alone would be fully written, so the context API's first two
+// steps run on the one-step kernel.
+constexpr int PT_BY = 30, PT_MZ = 64;
+constexpr unsigned PT_MPLANE = PT_MZ * PX_BY;
+template <int PB>
+struct PlumeTB {
+    static constexpr unsigned C_BYTES = PB * PX_PLANE;
+    static constexpr unsigned M_OFF = (C_BYTES + 127) / 128 * 128;
+    static constexpr unsigned M_BYTES = PB * PT_MPLANE;
+    static constexpr unsigned STAGE = (M_OFF + M_BYTES + 127) / 128 * 128;
+    static constexpr unsigned SMEM = PX_STAGES * STAGE;
+};
+
+struct PlumeW {
+    float w0, wx, wy, wb, wt, decay;
+};
+
+// One voxel's FTCS update from its neighbours and mask byte (the expression of every plume kernel);
+// FAST: the caller has established that if the voxel is updated all six neighbours are void.
+template <bool FAST>
+__device__ __forceinline__ float ftcs(float c0, float w, float e, float s, float n, float b, float t, unsigned m,
+                                      const PlumeW& k) {
+    if (!FAST) {
+        w = (m & 0x01) ? w : c0;
+        e = (m & 0x02) ? e : c0;
+        s = (m & 0x04) ? s : c0;
+        n = (m & 0x08) ? n : c0;
+        b = (m & 0x10) ? b : c0;
+        t = (m & 0x20) ? t : c0;
+    }
+    const float u = fmaxf((k.w0 * c0 + k.wx * (w + e) + k.wy * (s + n) + k.wb * b + k.wt * t) * k.decay, 0.0f);
+    return (m & BD_PM_UPDATE) ? u : 0.0f;
+}
+
+// true when every voxel of the byte set `m` that is updated has all six neighbours void
+__device__ __forceinline__ bool all_interior(unsigned m) {
+    const unsigned upd = (m >> 7) & 0x01010101u;
+    return (m & (upd * 0x3Fu)) == upd * 0x3Fu;
+}
+
+template <int PB>
+__global__ void __launch_bounds__(PX_THREADS, 1) k_plume_tb(const __grid_constant__ CUtensorMap c_map,
+                                                         const __grid_constant__ CUtensorMap m_map,
+                                                         float* __restrict__ Cn, int nx, int ny, int nz, PlumeConst c,
+                                                         const int* __restrict__ zlimit, int* __restrict__ err) {
+    using X = PlumeTB<PB>;
+    extern __shared__ __align__(128) unsigned char ring[];
+    __shared__ __align__(8) unsigned long long full[PX_STAGES], empty[PX_STAGES];
+    __shared__ volatile int s_fail;
+    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
+    const int n_kt = (zl + PL_BZ - 1) / PL_BZ;
+    const long long total = (long long)n_kt * ((ny + PT_BY - 1) / PT_BY) * nx;
+    const PlumeRun run{n_kt, PT_BY, nx, total * blockIdx.x / gridDim.x, total * (blockIdx.x + 1) / gridDim.x};
+    if (run.s0 >= run.s1) return;  // uniform over the CTA
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        for (int q = 0; q < PX_STAGES; ++q) {
+            mbar_init(&full[q], 1);
+            mbar_init(&empty[q], PX_NW);
+        }
+        mbar_init_fence();
+        s_fail = 0;
+    }
+    __syncthreads();
+    int issued = 0;
+    if (warp == PX_NW) {
+        // ---- producer warp (one lane): planes ib-2 .. ie+1 of each segment, PB per load ----
+        if (lane == 0) {
+            for (long long pos = run.s0; pos < run.s1 && !s_fail;) {
+                const int4 t = run.segment(pos);
+                pos += t.w - t.z;
+                const int nb = (t.w - t.z + 4 + PB - 1) / PB;
+                for (int b = 0; b < nb; ++b) {
+                    const int sl = issued & (PX_STAGES - 1);
+                    if (issued >= PX_STAGES && !mbar_wait(&empty[sl], ((issued / PX_STAGES) - 1) & 1)) {
+                        s_fail = 1;
+                        break;
+                    }
+                    mbar_expect_tx(&full[sl], X::C_BYTES + X::M_BYTES);
+                    unsigned char* st = ring + sl * X::STAGE;
+                    tma_load_3d(st, &c_map, t.x - 4, t.y - 2, t.z - 2 + PB * b, &full[sl]);
+                    tma_load_3d(st + X::M_OFF, &m_map, t.x - 16, t.y - 1, t.z - 2 + PB * b, &full[sl]);
+                    ++issued;
+                }
+            }
+        }
+    } else {
+        // ---- consumer warps: warp = z group, lane = row y = j0 - 1 + lane ----
+        PlumeW kw;
+        kw.wx = c.dtp * c.dxy_x; kw.wy = c.dtp * c.dxy_y; kw.wb = c.dtp * c.dz_z;
+        kw.wt = kw.wb + c.dtp * c.vz_over_dz;
+        kw.w0 = 1.0f - 2.0f * (kw.wx + kw.wy + kw.wb) - c.dtp * c.vz_over_dz;
+        kw.decay = c.decay;
+        const int plane = ny * nz;
+        const int t0 = (lane + 1) * PX_PZ + 4 + 4 * warp;          // own row, z = k (16-byte aligned)
+        const int mo = X::M_OFF + lane * PT_MZ + 16 + 4 * warp;    // own mask bytes, z = k
+        int L = 0;
+        bool ok = true;
+        for (long long pos = run.s0; pos < run.s1 && ok;) {
+            const int4 t = run.segment(pos);
+            const int k0 = t.x, j0 = t.y, ib = t.z, ie = t.w;
+            pos += ie - ib;
+            const int np = ie - ib + 4, nb = (np + PB - 1) / PB;  // planes ib-2 .. ie+1 in nb loads
+            const int k = k0 + 4 * warp;
+            // mask bytes of z = k-1 .. k+4 that lie at or below zl are cleared (not rebuilt there)
+            const int nk = zl - k;
+            const unsigned zkeep = nk >= 4 ? 0xffffffffu : (nk <= 0 ? 0u : (0xffffffffu >> (8 * (4 - nk))));
+            const bool lo_ok = k >= 1 && k - 1 < zl, hi_ok = k + 4 < zl;
+            const bool store = lane >= 1 && lane <= PT_BY && j0 - 1 + lane < ny && nk > 0;
+            float* dst = Cn + (size_t)ib * plane + (size_t)(j0 - 1 + lane) * nz + k;
+            int waited = 0, released = 0;
+#define BD_PT_PLANE(q) (ring + ((L + (q) / PB) & (PX_STAGES - 1)) * X::STAGE + ((q) % PB) * PX_PLANE)
+#define BD_PT_MASK(q) (ring + ((L + (q) / PB) & (PX_STAGES - 1)) * X::STAGE + mo + ((q) % PB) * PT_MPLANE)
+            // C0 of planes q-2, q-1 and C1 of planes q-3, q-2 (x-rotation), z = k-1 .. k+4
+            float a0[6], a1[6], b0[6], b1[6];
+            unsigned mprev = 0;  // mask bytes z = k .. k+3 of the plane C2 is computed on
+#pragma unroll
+            for (int e = 0; e < 6; ++e) a0[e] = a1[e] = b0[e] = b1[e] = 0.0f;
+            for (int q = 0; q < np; ++q) {
+                while (ok && waited <= q / PB) {
+                    if (!px_wait(full, L + waited, &s_fail)) ok = false;
+                    ++waited;
+                }
+                if (!ok) break;
+                float a2[6];
+                {
+                    const float* tq = reinterpret_cast<const float*>(BD_PT_PLANE(q));
+                    const float4 v = *reinterpret_cast<const float4*>(tq + t0);
+                    a2[0] = tq[t0 - 1]; a2[1] = v.x; a2[2] = v.y; a2[3] = v.z; a2[4] = v.w; a2[5] = tq[t0 + 4];
+                }
+                float b2[6];
+#pragma unroll
+                for (int e = 0; e < 6; ++e) b2[e] = 0.0f;
+                unsigned mcur = 0;
+                if (q >= 2) {
+                    // ---- first step on plane q-1 (centre), z = k-1 .. k+4 ----
+                    const unsigned char* mq = BD_PT_MASK(q - 1);
+                    mcur = *reinterpret_cast<const unsigned*>(mq) & zkeep;
+                    const unsigned mlo = lo_ok ? mq[-1] : 0u, mhi = hi_ok ? mq[4] : 0u;
+                    const bool live = __any_sync(0xffffffffu, ((mcur | mlo | mhi) & 0x40404040u) != 0);
+                    if (live) {
+                        const float* tc = reinterpret_cast<const float*>(BD_PT_PLANE(q - 1));
+                        const float4 sv = *reinterpret_cast<const float4*>(tc + t0 - PX_PZ);
+                        const float4 nv = *reinterpret_cast<const float4*>(tc + t0 + PX_PZ);
+                        const float s6[6] = {tc[t0 - PX_PZ - 1], sv.x, sv.y, sv.z, sv.w, tc[t0 - PX_PZ + 4]};
+                        const float n6[6] = {tc[t0 + PX_PZ - 1], nv.x, nv.y, nv.z, nv.w, tc[t0 + PX_PZ + 4]};
+                        const float zm = tc[t0 - 2], zp = tc[t0 + 5];
+                        const unsigned m6[6] = {mlo, mcur & 0xffu, (mcur >> 8) & 0xffu, (mcur >> 16) & 0xffu,
+                                                mcur >> 24, mhi};
+                        const bool fast = all_interior(mcur) && all_interior(mlo) && all_interior(mhi);
+                        if (__all_sync(0xffffffffu, fast)) {
+#pragma unroll
+                            for (int e = 0; e < 6; ++e)
+                                b2[e] = ftcs<true>(a1[e], a0[e], a2[e], s6[e], n6[e], e > 0 ? a1[e - 1] : zm,
+                                                   e < 5 ? a1[e + 1] : zp, m6[e], kw);
+                        } else {
+#pragma unroll
+                            for (int e = 0; e < 6; ++e)
+                                b2[e] = ftcs<false>(a1[e], a0[e], a2[e], s6[e], n6[e], e > 0 ? a1[e - 1] : zm,
+                                                    e < 5 ? a1[e + 1] : zp, m6[e], kw);
+                        }
+                    }
+                }
+                // the smem of plane q-1 has been read for the last time: release its load when it was
+                // the load's last plane
+                if (q >= 1 && q % PB == 0) {
+                    px_release(empty, L + released, lane);
+                    ++released;
+                }
+                if (q >= 4) {
+                    // ---- second step on plane q-2 = x ib-4+q, z = k .. k+3, from C1 of planes q-3 .. q-1 ----
+                    float sy[4], ny4[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        sy[e] = __shfl_up_sync(0xffffffffu, b1[e + 1], 1);
+                        ny4[e] = __shfl_down_sync(0xffffffffu, b1[e + 1], 1);
+                    }
+                    const unsigned vd = mprev & 0x40404040u;
+                    if (__any_sync(0xffffffffu, store && vd != 0)) {
+                        float v[4];
+                        if (__all_sync(0xffffffffu, !store || all_interior(mprev))) {
+#pragma unroll
+                            for (int e = 0; e < 4; ++e)
+                                v[e] = ftcs<true>(b1[e + 1], b0[e + 1], b2[e + 1], sy[e], ny4[e], b1[e], b1[e + 2],
+                                                  (mprev >> (8 * e)) & 0xffu, kw);
+                        } else {
+#pragma unroll
+                            for (int e = 0; e < 4; ++e)
+                                v[e] = ftcs<false>(b1[e + 1], b0[e + 1], b2[e + 1], sy[e], ny4[e], b1[e], b1[e + 2],
+                                                   (mprev >> (8 * e)) & 0xffu, kw);
+                        }
+                        if (store && vd) {
+                            if (vd == 0x40404040u) {
+                                *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+                            } else {
+#pragma unroll
+                                for (int e = 0; e < 4; ++e)
+                                    if (vd & (0x40u << (8 * e))) dst[e] = v[e];
+                            }
+                        }
+                    }
+                    dst += plane;
+                }
+#pragma unroll
+                for (int e = 0; e < 6; ++e) {
+                    a0[e] = a1[e]; a1[e] = a2[e];
+                    b0[e] = b1[e]; b1[e] = b2[e];
+                }
+                mprev = mcur;
+            }
+            if (!ok) break;
+            for (; released < nb; ++released) px_release(empty, L + released, lane);
+            L += nb;
+#undef BD_PT_PLANE
+#undef BD_PT_MASK
+        }
+    }
+    __syncthreads();
+    if (tid == PX_NW * 32 && s_fail) {
+        atomicExch(err, 1);
         for (int q = max(0, issued - PX_STAGES); q < issued; ++q)
             mbar_wait(&full[q & (PX_STAGES - 1)], (q / PX_STAGES) & 1);
     }
@@ -888,9 +1122,11 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
 #ifdef BD_NO_TMA
     err = nullptr;
 #endif
-    // plume kernel: 0 = scalar TMA kernel, 1 / 2 = persistent x-marching kernel, 2 / 4 planes per copy
+    // plume kernel: 0 = scalar TMA kernel, 1 / 2 = persistent x-marching kernel, 2 / 4 planes per copy,
+    // 3 = two steps per launch (k_plume_tb, 2 planes per copy; single steps on kernel 1)
     // (one CTA per SM register budget: 64 registers x 288 threads, so at most 3 CTAs per SM)
-    const int shape = tune_value(BD_TUNE_PLUME_KERNEL);
+    const int kernel = tune_value(BD_TUNE_PLUME_KERNEL);
+    const int shape = kernel == 3 ? 1 : kernel;  // the one-step kernel
     const int pb = shape == 1 ? 2 : 4;
     const int py = shape == 0 ? PL_PY : PX_PY;
     const int pz = shape == 0 ? PL_PZ : PX_PZ;
@@ -898,10 +1134,12 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     const bool tma = err != nullptr && make_tmap_3d_f32(&map_a, Ca, p->nx, p->ny, p->nz, pz, py, bx) &&
                      make_tmap_3d_f32(&map_b, Cb, p->nx, p->ny, p->nz, pz, py, bx) &&
                      (shape == 0 || make_tmap_3d_u8(&map_m, mask, p->nx, p->ny, p->nz, mz, PL_BZ, PX_BY, pb));
+    CUtensorMap map_m2;
+    const bool two = tma && kernel == 3 && make_tmap_3d_u8(&map_m2, mask, p->nx, p->ny, p->nz, mz, PT_MZ, PX_BY, 2);
     const int xc = tune_value(BD_TUNE_PLUME_XC);
     const dim3 tgrid((p->nz + PL_BZ - 1) / PL_BZ, (p->ny + PL_BY - 1) / PL_BY, (p->nx + xc - 1) / xc);
-    // persistent kernel: xc CTAs per SM (capped by occupancy), at most one per plane of the grid
-    int xm_grid = 0;
+    // persistent kernels: xc CTAs per SM (capped by occupancy), at most one per plane tile of the grid
+    int xm_grid = 0, tb_grid = 0;
     unsigned xm_smem = shape == 1 ? PlumeXM<2>::SMEM : PlumeXM<4>::SMEM;
     if (tma && shape > 0) {
         int dev = 0, sms = 0, occ = 0;
@@ -917,14 +1155,33 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
         const long long planes =
             (long long)((p->nz + PL_BZ - 1) / PL_BZ) * ((p->ny + PX_BY - 1) / PX_BY) * p->nx;
         xm_grid = (int)std::max(1LL, std::min(planes, (long long)std::max(std::min(occ, xc), 1) * sms));
+        if (two) {
+            int occ2 = 0;
+            BD_CUDA(cudaFuncSetAttribute(k_plume_tb<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         PlumeTB<2>::SMEM));
+            BD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_plume_tb<2>, PX_THREADS, PlumeTB<2>::SMEM));
+            const long long planes2 =
+                (long long)((p->nz + PL_BZ - 1) / PL_BZ) * ((p->ny + PT_BY - 1) / PT_BY) * p->nx;
+            tb_grid = (int)std::max(1LL, std::min(planes2, (long long)std::max(std::min(occ2, xc), 1) * sms));
+        }
     }
     const long long total = (long long)steps * n_substeps;
-    for (long long s = 0; s < total; ++s) {
-        const float* in = (s & 1) ? Cb : Ca;
-        float* out = (s & 1) ? Ca : Cb;
+    long long launches = 0;  // each launch moves the field to the other buffer
+    for (long long s = 0; s < total;) {
+        const bool odd = launches & 1;
+        const float* in = odd ? Cb : Ca;
+        float* out = odd ? Ca : Cb;
         const int full = (full_first && s < 2) ? 1 : 0;
-        const CUtensorMap& map = (s & 1) ? map_b : map_a;
+        const CUtensorMap& map = odd ? map_b : map_a;
         const int* zl = full ? nullptr : zlimit;
+        ++launches;
+        if (two && !full && total - s >= 2) {
+            k_plume_tb<2><<<tb_grid, PX_THREADS, PlumeTB<2>::SMEM, st>>>(map, map_m2, out, p->nx, p->ny, p->nz, c, zl,
+                                                                       err);
+            s += 2;
+            continue;
+        }
+        ++s;
         if (tma && shape == 1)
             k_plume_xm<2><<<xm_grid, PX_THREADS, xm_smem, st>>>(map, map_m, out, p->nx, p->ny, p->nz, c, zl, full, err);
         else if (tma && shape == 2)
@@ -937,7 +1194,7 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
                                                         full ? nullptr : zlimit, full);
     }
     BD_CHECK_LAUNCH("k_plume_step");
-    if (in_b) *in_b = (int)(total & 1);
+    if (in_b) *in_b = (int)(launches & 1);
     return BD_OK;
 }
 }  // namespace bd

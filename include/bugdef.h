@@ -358,7 +358,7 @@ BD_API int bd_engine_record(BdEngine* e, const BdRecordSpec* spec, void* slot, v
                                         occupancy); 1..64 (default 4)                                  */
 #define BD_TUNE_PLUME_KERNEL      3  /* plume step: 0 = one voxel per thread, x chunks per CTA; 1 / 2 =
                                         persistent, four z voxels per thread marching x, 2 / 4 x-planes
-                                        per copy (default 1)                                           */
+                                        per copy; 3 = as 1 with two time steps per launch (default 1)  */
 #define BD_TUNE_COUNT             4
 BD_API int bd_tune_set(int knob, int value);
 BD_API int bd_tune_get(int knob, int* value);
