@@ -283,6 +283,11 @@ def ours_main(args):
     dom = "substeps" if stage[1] >= stage[2] else "plume"
     bytes_per_launch = ab["substep"] if dom == "substeps" else ab["plume_step"]
     achieved = bytes_per_launch / (per_launch[dom] * 1e-3) / 1e9
+    from bug_defense_b200 import _lib
+    kv = ctypes.c_int(0)
+    _lib.call("bd_tune_get", _lib.TUNE_PLUME_KERNEL, ctypes.byref(kv))
+    plume_kernel = {0: "k_plume_step_tma", 1: "k_plume_xm<2>", 2: "k_plume_xm<4>",
+                    3: "k_plume_tb<2>"}.get(kv.value, "k_plume_step")
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
@@ -290,10 +295,6 @@ def ours_main(args):
         key = {"substeps": "k_substep", "plume": plume_kernel.split("<")[0]}[dom]
         if key in tj:
             traffic = tj[key]["bytes_per_voxel"] * eng.Nx * eng.Ny * eng.Nz
-    from bug_defense_b200 import _lib
-    kv = ctypes.c_int(0)
-    _lib.call("bd_tune_get", _lib.TUNE_PLUME_KERNEL, ctypes.byref(kv))
-    plume_kernel = {0: "k_plume_step_tma", 1: "k_plume_xm<2>", 2: "k_plume_xm<4>"}.get(kv.value, "k_plume_step")
     roof = {"bound": "hbm", "kernel": {"substeps": "k_substep<fused ablation>", "plume": plume_kernel}[dom],
             "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
             "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
