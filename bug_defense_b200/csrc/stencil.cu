@@ -526,6 +526,33 @@ __device__ __forceinline__ void px_release(unsigned long long* empty, int q, int
     if (lane == 0) mbar_arrive(&empty[q & (PX_STAGES - 1)]);
 }
 
+struct PlumeW {
+    float w0, wx, wy, wb, wt, decay;
+};
+
+// One voxel's FTCS update from its neighbours and mask byte (the expression of every plume kernel);
+// FAST: the caller has established that if the voxel is updated all six neighbours are void.
+template <bool FAST>
+__device__ __forceinline__ float ftcs(float c0, float w, float e, float s, float n, float b, float t, unsigned m,
+                                      const PlumeW& k) {
+    if (!FAST) {
+        w = (m & 0x01) ? w : c0;
+        e = (m & 0x02) ? e : c0;
+        s = (m & 0x04) ? s : c0;
+        n = (m & 0x08) ? n : c0;
+        b = (m & 0x10) ? b : c0;
+        t = (m & 0x20) ? t : c0;
+    }
+    const float u = fmaxf((k.w0 * c0 + k.wx * (w + e) + k.wy * (s + n) + k.wb * b + k.wt * t) * k.decay, 0.0f);
+    return (m & BD_PM_UPDATE) ? u : 0.0f;
+}
+
+// true when every voxel of the byte set `m` that is updated has all six neighbours void
+__device__ __forceinline__ bool all_interior(unsigned m) {
+    const unsigned upd = (m >> 7) & 0x01010101u;
+    return (m & (upd * 0x3Fu)) == upd * 0x3Fu;
+}
+
 template <int PB>
 __global__ void __launch_bounds__(PX_THREADS, 1) k_plume_xm(const __grid_constant__ CUtensorMap c_map,
                                                          const __grid_constant__ CUtensorMap m_map,
@@ -575,9 +602,11 @@ __global__ void __launch_bounds__(PX_THREADS, 1) k_plume_xm(const __grid_constan
         }
     } else {
         // ---- consumer warps: warp = z group, lane = tile row ----
-        const float wx = c.dtp * c.dxy_x, wy = c.dtp * c.dxy_y, wb = c.dtp * c.dz_z;
-        const float wt = wb + c.dtp * c.vz_over_dz;
-        const float w0 = 1.0f - 2.0f * (wx + wy + wb) - c.dtp * c.vz_over_dz;
+        PlumeW kw;
+        kw.wx = c.dtp * c.dxy_x; kw.wy = c.dtp * c.dxy_y; kw.wb = c.dtp * c.dz_z;
+        kw.wt = kw.wb + c.dtp * c.vz_over_dz;
+        kw.w0 = 1.0f - 2.0f * (kw.wx + kw.wy + kw.wb) - c.dtp * c.vz_over_dz;
+        kw.decay = c.decay;
         const int plane = ny * nz;
         const int t0 = (lane + 1) * PX_PZ + 4 + 4 * warp;  // this thread's float4 in a plane (16-byte aligned)
         const int mo = X::M_OFF + lane * PL_BZ + 4 * warp;  // its four mask bytes in mask plane 0
@@ -619,42 +648,22 @@ __global__ void __launch_bounds__(PX_THREADS, 1) k_plume_xm(const __grid_constan
                 const unsigned vd = mr & 0x40404040u;  // void bit of each of the four voxels
                 // every voxel that is updated has all six neighbours void (outer-wall and tissue voxels,
                 // not updated, take 0 as on the general path)
-                const unsigned upd = (mr >> 7) & 0x01010101u;
-                const bool bulk = (mr & (upd * 0x3Fu)) == upd * 0x3Fu;
+                const bool bulk = all_interior(mr);
                 if (__any_sync(0xffffffffu, act && (vd || full_write))) {
                     const float4 cs = *reinterpret_cast<const float4*>(tc + t0 - PX_PZ);
                     const float4 cn = *reinterpret_cast<const float4*>(tc + t0 + PX_PZ);
                     const float zb = tc[t0 - 1], zt = tc[t0 + 4];
                     float v[4];
                     if (__all_sync(0xffffffffu, bulk || !act)) {
-                        v[0] = fmaxf((w0 * cc.x + wx * (cw.x + ce.x) + wy * (cs.x + cn.x) + wb * zb + wt * cc.y) * c.decay, 0.0f);
-                        v[1] = fmaxf((w0 * cc.y + wx * (cw.y + ce.y) + wy * (cs.y + cn.y) + wb * cc.x + wt * cc.z) * c.decay, 0.0f);
-                        v[2] = fmaxf((w0 * cc.z + wx * (cw.z + ce.z) + wy * (cs.z + cn.z) + wb * cc.y + wt * cc.w) * c.decay, 0.0f);
-                        v[3] = fmaxf((w0 * cc.w + wx * (cw.w + ce.w) + wy * (cs.w + cn.w) + wb * cc.z + wt * zt) * c.decay, 0.0f);
-#pragma unroll
-                        for (int e = 0; e < 4; ++e) v[e] = ((upd >> (8 * e)) & 1u) ? v[e] : 0.0f;
+                        v[0] = ftcs<true>(cc.x, cw.x, ce.x, cs.x, cn.x, zb, cc.y, mr & 0xffu, kw);
+                        v[1] = ftcs<true>(cc.y, cw.y, ce.y, cs.y, cn.y, cc.x, cc.z, (mr >> 8) & 0xffu, kw);
+                        v[2] = ftcs<true>(cc.z, cw.z, ce.z, cs.z, cn.z, cc.y, cc.w, (mr >> 16) & 0xffu, kw);
+                        v[3] = ftcs<true>(cc.w, cw.w, ce.w, cs.w, cn.w, cc.z, zt, mr >> 24, kw);
                     } else {
-                        const float c0v[4] = {cc.x, cc.y, cc.z, cc.w};
-                        const float cwv[4] = {cw.x, cw.y, cw.z, cw.w};
-                        const float cev[4] = {ce.x, ce.y, ce.z, ce.w};
-                        const float csv[4] = {cs.x, cs.y, cs.z, cs.w};
-                        const float cnv[4] = {cn.x, cn.y, cn.z, cn.w};
-                        const float cbv[4] = {zb, cc.x, cc.y, cc.z};
-                        const float ctv[4] = {cc.y, cc.z, cc.w, zt};
-#pragma unroll
-                        for (int e = 0; e < 4; ++e) {
-                            const unsigned me = mr >> (8 * e);
-                            const float c0 = c0v[e];
-                            const float w = (me & 0x01) ? cwv[e] : c0;
-                            const float ee = (me & 0x02) ? cev[e] : c0;
-                            const float sx = (me & 0x04) ? csv[e] : c0;
-                            const float nn = (me & 0x08) ? cnv[e] : c0;
-                            const float b = (me & 0x10) ? cbv[e] : c0;
-                            const float tz = (me & 0x20) ? ctv[e] : c0;
-                            const float u =
-                                fmaxf((w0 * c0 + wx * (w + ee) + wy * (sx + nn) + wb * b + wt * tz) * c.decay, 0.0f);
-                            v[e] = (me & BD_PM_UPDATE) ? u : 0.0f;
-                        }
+                        v[0] = ftcs<false>(cc.x, cw.x, ce.x, cs.x, cn.x, zb, cc.y, mr & 0xffu, kw);
+                        v[1] = ftcs<false>(cc.y, cw.y, ce.y, cs.y, cn.y, cc.x, cc.z, (mr >> 8) & 0xffu, kw);
+                        v[2] = ftcs<false>(cc.z, cw.z, ce.z, cs.z, cn.z, cc.y, cc.w, (mr >> 16) & 0xffu, kw);
+                        v[3] = ftcs<false>(cc.w, cw.w, ce.w, cs.w, cn.w, cc.z, zt, mr >> 24, kw);
                     }
                     if (act && (vd || full_write)) {
                         if (full_write || vd == 0x40404040u) {
@@ -711,33 +720,6 @@ struct PlumeTB {
     static constexpr unsigned STAGE = (M_OFF + M_BYTES + 127) / 128 * 128;
     static constexpr unsigned SMEM = PX_STAGES * STAGE;
 };
-
-struct PlumeW {
-    float w0, wx, wy, wb, wt, decay;
-};
-
-// One voxel's FTCS update from its neighbours and mask byte (the expression of every plume kernel);
-// FAST: the caller has established that if the voxel is updated all six neighbours are void.
-template <bool FAST>
-__device__ __forceinline__ float ftcs(float c0, float w, float e, float s, float n, float b, float t, unsigned m,
-                                      const PlumeW& k) {
-    if (!FAST) {
-        w = (m & 0x01) ? w : c0;
-        e = (m & 0x02) ? e : c0;
-        s = (m & 0x04) ? s : c0;
-        n = (m & 0x08) ? n : c0;
-        b = (m & 0x10) ? b : c0;
-        t = (m & 0x20) ? t : c0;
-    }
-    const float u = fmaxf((k.w0 * c0 + k.wx * (w + e) + k.wy * (s + n) + k.wb * b + k.wt * t) * k.decay, 0.0f);
-    return (m & BD_PM_UPDATE) ? u : 0.0f;
-}
-
-// true when every voxel of the byte set `m` that is updated has all six neighbours void
-__device__ __forceinline__ bool all_interior(unsigned m) {
-    const unsigned upd = (m >> 7) & 0x01010101u;
-    return (m & (upd * 0x3Fu)) == upd * 0x3Fu;
-}
 
 template <int PB>
 __global__ void __launch_bounds__(PX_THREADS, 1) k_plume_tb(const __grid_constant__ CUtensorMap c_map,
@@ -1124,7 +1106,7 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
 #endif
     // plume kernel: 0 = scalar TMA kernel, 1 / 2 = persistent x-marching kernel, 2 / 4 planes per copy,
     // 3 = two steps per launch (k_plume_tb, 2 planes per copy; single steps on kernel 1)
-    // (one CTA per SM register budget: 64 registers x 288 threads, so at most 3 CTAs per SM)
+    // (64 registers x 288 threads: at most 3 CTAs per SM; 4 at 56 registers measured slower)
     const int kernel = tune_value(BD_TUNE_PLUME_KERNEL);
     const int shape = kernel == 3 ? 1 : kernel;  // the one-step kernel
     const int pb = shape == 1 ? 2 : 4;
