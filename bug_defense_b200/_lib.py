@@ -101,6 +101,7 @@ class PlumeParams(Structure):
 FLAG_NEWLY = 0x08
 EPOCH_SKIP_MC = 0x1
 EPOCH_NO_GRAPH = 0x2
+EPOCH_SERIAL_PLUME = 0x4
 
 
 class GridRef(Structure):

@@ -374,9 +374,15 @@ class CoupledAblationEngine:
         self._enqueue(opts)
         return self._diag(absorbed_map)
 
+    # run the plume stage after the substeps on the caller's stream instead of beside MC + substeps
+    # on the engine's own plume stream (same results; the stages share no data within an epoch)
+    serial_plume = False
+
     def _enqueue(self, opts=0):
         if not self.use_graphs:
             opts |= _lib.EPOCH_NO_GRAPH
+        if self.serial_plume:
+            opts |= _lib.EPOCH_SERIAL_PLUME
         _lib.call("bd_engine_step_epoch", self._handle, float(self._power), int(opts), _lib.stream_ptr())
         self._last_power = self._power
 

@@ -22,6 +22,11 @@ struct StageGraph {
 struct BdEngine {
     BdEngineDesc d;
     cudaStream_t cap_stream = nullptr;  // private stream used only to capture stage graphs
+    // the plume stage runs on its own (higher-priority) stream, forked after the epoch begins and
+    // joined before the epoch end: within an epoch it shares no data with the MC and the substeps
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool ring_concurrent = false;  // the timing ring's plume events come from the side stream
     StageGraph g_mc, g_sub_on, g_sub_off, g_plume, g_end;
     uint8_t* plume_mask = nullptr;      // plume neighbourhood bytes (rebuilt every epoch)
     bd::PhaseArgs pa;
@@ -208,6 +213,13 @@ extern "C" int bd_engine_create(const BdEngineDesc* desc, BdEngine** out) {
     if (err == cudaSuccess) err = cudaMemset(e->dyn, 0, sizeof(EngineDyn));
     for (int q = 0; q < 4 && err == cudaSuccess; ++q) err = cudaEventCreate(&e->ev[q]);
     if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->cap_stream, cudaStreamNonBlocking);
+    if (err == cudaSuccess && desc->has_plume_transport) {
+        int lo = 0, hi = 0;
+        err = cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        if (err == cudaSuccess) err = cudaStreamCreateWithPriority(&e->side, cudaStreamNonBlocking, hi);
+        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming);
+        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming);
+    }
     if (err == cudaSuccess && desc->has_plume_transport)
         err = cudaMalloc(&e->plume_mask, plume_mask_bytes(desc->phase.nx, desc->phase.ny, desc->phase.nz));
     if (err != cudaSuccess) {
@@ -243,6 +255,9 @@ extern "C" int bd_engine_destroy(BdEngine* e) {
     graph_reset(e->g_mc); graph_reset(e->g_sub_on); graph_reset(e->g_sub_off);
     graph_reset(e->g_plume); graph_reset(e->g_end);
     if (e->cap_stream) cudaStreamDestroy(e->cap_stream);
+    if (e->side) cudaStreamDestroy(e->side);
+    if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+    if (e->ev_join) cudaEventDestroy(e->ev_join);
     cudaFree(e->plume_mask);
     delete e;
     return BD_OK;
@@ -276,6 +291,38 @@ extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void*
 
     const bool laser = power > 0.0f;
     int rc = BD_OK;
+    const bool plume = d.n_substeps > 0 && d.has_plume_transport;
+    const bool conc = plume && e->side && !(options & BD_EPOCH_SERIAL_PLUME);
+    auto plume_stage = [&](cudaStream_t on) -> int {
+        return run_stage(e, e->g_plume, &d.plume, sizeof(d.plume), graphs, on, [&](cudaStream_t s) -> int {
+            int in_b = 0;
+            int r = plume_launch(&d.plume, d.phase.plume, d.plume_alt, d.n_substeps, d.phase.flags, &in_b, s,
+                                 &e->dyn->void_zlimit, 0, e->plume_mask, &e->dyn->err);
+            if (r) return r;
+            if (in_b)
+                BD_CUDA(cudaMemcpyAsync(d.phase.plume, d.plume_alt, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
+            return BD_OK;
+        });
+    };
+    // ring slots 1..3 (after MC, after substeps, after plume) are reserved up front when the plume
+    // runs concurrently, so the ring keeps its per-epoch order
+    cudaEvent_t r_mc = nullptr, r_sub = nullptr, r_pl = nullptr;
+    if (conc) {
+        if (e->ring_on && e->timed) {
+            r_mc = ring_event(e);
+            r_sub = ring_event(e);
+            r_pl = ring_event(e);
+            e->ring_concurrent = true;
+        }
+        BD_CUDA(cudaEventRecord(e->ev_fork, st));
+        BD_CUDA(cudaStreamWaitEvent(e->side, e->ev_fork, 0));
+        rc = plume_stage(e->side);
+        if (rc) return rc;
+        if (r_pl) cudaEventRecord(r_pl, e->side);
+        BD_CUDA(cudaEventRecord(e->ev_join, e->side));
+    } else if (e->ring_on && e->timed) {
+        e->ring_concurrent = false;
+    }
     if (laser && !(options & BD_EPOCH_SKIP_MC)) {
         BD_REQUIRE(d.phase.props != nullptr, "bd_engine_step_epoch: MC needs the packed property buffer");
         BdMcParams mp = d.mc;
@@ -288,7 +335,12 @@ extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void*
         });
         if (rc) return rc;
     }
-    mark(e, st, 1);
+    if (conc) {
+        if (e->timed) cudaEventRecord(e->ev[1], st);
+        if (r_mc) cudaEventRecord(r_mc, st);
+    } else {
+        mark(e, st, 1);
+    }
     if (d.n_substeps > 0) {
         BdAblationParams ap = d.substep;
         ap.is_active = laser ? 1 : 0;
@@ -305,20 +357,18 @@ extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void*
         });
         if (rc) return rc;
     }
-    mark(e, st, -1);
-    if (d.n_substeps > 0 && d.has_plume_transport) {
-        rc = run_stage(e, e->g_plume, &d.plume, sizeof(d.plume), graphs, st, [&](cudaStream_t s) -> int {
-            int in_b = 0;
-            int r = plume_launch(&d.plume, d.phase.plume, d.plume_alt, d.n_substeps, d.phase.flags, &in_b, s,
-                                 &e->dyn->void_zlimit, 0, e->plume_mask, &e->dyn->err);
-            if (r) return r;
-            if (in_b)
-                BD_CUDA(cudaMemcpyAsync(d.phase.plume, d.plume_alt, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
-            return BD_OK;
-        });
-        if (rc) return rc;
+    if (conc) {
+        if (r_sub) cudaEventRecord(r_sub, st);
+        BD_CUDA(cudaStreamWaitEvent(st, e->ev_join, 0));
+        if (e->timed) cudaEventRecord(e->ev[2], st);
+    } else {
+        mark(e, st, -1);
+        if (plume) {
+            rc = plume_stage(st);
+            if (rc) return rc;
+        }
+        mark(e, st, 2);
     }
-    mark(e, st, 2);
     rc = run_stage(e, e->g_end, &e->pa, sizeof(e->pa), graphs, st, [&](cudaStream_t s) -> int {
         return phase_launch(e->pa, BD_PHASE_FULL, s);
     });
@@ -388,12 +438,24 @@ extern "C" int bd_engine_timing_read(BdEngine* e, double* stage_ms, int64_t* epo
     *epochs = (int64_t)n;
     if (n == 0) return BD_OK;
     BD_CUDA(cudaEventSynchronize(e->ring[e->ring_used - 1]));
-    for (size_t ep = 0; ep < n; ++ep)
-        for (int q = 0; q < 4; ++q) {
-            float ms = 0.0f;
-            BD_CUDA(cudaEventElapsedTime(&ms, e->ring[ep * 5 + q], e->ring[ep * 5 + q + 1]));
-            stage_ms[q] += ms;
+    for (size_t ep = 0; ep < n; ++ep) {
+        cudaEvent_t* r = &e->ring[ep * 5];  // begin, after MC, after substeps, after plume, after end
+        float ms[4] = {0.f, 0.f, 0.f, 0.f};
+        BD_CUDA(cudaEventElapsedTime(&ms[0], r[0], r[1]));
+        BD_CUDA(cudaEventElapsedTime(&ms[1], r[1], r[2]));
+        if (e->ring_concurrent) {
+            // the plume ran beside MC + substeps from the epoch begin; the epoch end starts after both
+            float a = 0.f, b = 0.f;
+            BD_CUDA(cudaEventElapsedTime(&ms[2], r[0], r[3]));
+            BD_CUDA(cudaEventElapsedTime(&a, r[2], r[4]));
+            BD_CUDA(cudaEventElapsedTime(&b, r[3], r[4]));
+            ms[3] = std::min(a, b);
+        } else {
+            BD_CUDA(cudaEventElapsedTime(&ms[2], r[2], r[3]));
+            BD_CUDA(cudaEventElapsedTime(&ms[3], r[3], r[4]));
         }
+        for (int q = 0; q < 4; ++q) stage_ms[q] += ms[q];
+    }
     return BD_OK;
 }
 

@@ -287,6 +287,8 @@ typedef struct BdEpochDiag {
 
 #define BD_EPOCH_SKIP_MC 0x1       /* use the absorbed map already in A (no MC this epoch) */
 #define BD_EPOCH_NO_GRAPH 0x2      /* launch the stages directly instead of as CUDA graphs  */
+#define BD_EPOCH_SERIAL_PLUME 0x4  /* run the plume stage after the substeps on the caller's stream
+                                      instead of beside MC + substeps on the engine's plume stream */
 
 typedef struct BdEngine BdEngine;
 /* Replaces CoupledAblationEngine.__init__ device setup (coupled_ablation.py:184-407);
