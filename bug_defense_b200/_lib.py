@@ -221,6 +221,7 @@ _SIGNATURES = {
     "bd_engine_record": (c_int, [c_void_p, POINTER(RecordSpec), c_void_p, c_void_p]),
     "bd_tune_set": (c_int, [c_int, c_int]),
     "bd_tune_get": (c_int, [c_int, POINTER(c_int)]),
+    "bd_selftest_wait_timeout": (c_int, [c_int, c_int, c_void_p]),
     "bd_conv_plane_rows": (c_int64, [c_int, c_int, c_int]),
     "bd_conv_image_bytes": (c_int64, [c_int, c_int, c_int]),
     "bd_conv_pack_weights": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),

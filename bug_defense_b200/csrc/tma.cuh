@@ -43,10 +43,10 @@ __device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
-// Bounded wait for the phase with the given parity; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+// Bounded wait for the phase with the given parity: at most `limit` polls; false on timeout.
+__device__ __forceinline__ bool mbar_wait_limit(unsigned long long* bar, unsigned parity, unsigned limit) {
     const unsigned a = smem_addr(bar);
-    for (unsigned it = 0; it < TMA_SPIN_LIMIT; ++it) {
+    for (unsigned it = 0; it < limit; ++it) {
         unsigned done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -58,6 +58,11 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
         if (done) return true;
     }
     return false;
+}
+
+// The kernels' wait: bounded by TMA_SPIN_LIMIT polls (about 4 s).
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    return mbar_wait_limit(bar, parity, TMA_SPIN_LIMIT);
 }
 
 // Orders this thread's earlier generic-proxy shared-memory accesses before later async-proxy

@@ -365,6 +365,12 @@ BD_API int bd_engine_record(BdEngine* e, const BdRecordSpec* spec, void* slot, v
 BD_API int bd_tune_set(int knob, int value);
 BD_API int bd_tune_get(int knob, int* value);
 
+/* Self-test of the bounded-wait failure path (no counterpart in the reference): one thread waits at
+ * most max_polls (1..2^20) polls, through the kernels' own bounded mbarrier wait, on a barrier that
+ * nothing arrives on (arrive = 0: returns BD_ERR_TIMEOUT) or that it completed itself (arrive = 1:
+ * BD_OK). Synchronises `stream`; the context stays usable after the timeout. */
+BD_API int bd_selftest_wait_timeout(int max_polls, int arrive, void* stream);
+
 /* ---------------------------------------------------------------------------------------------
  * Absorbed-map denoiser: 3-D convolution layers (tcgen05 BF16 tensor cores, FP32 accumulation).
  * No counterpart in the reference, which has no learned component; these are the building blocks
