@@ -42,6 +42,9 @@ def to_dev(a, dev, dtype=torch.float32) -> torch.Tensor:
     if isinstance(a, torch.Tensor):
         return a.to(device=dev, dtype=dtype).contiguous()
     arr = np.ascontiguousarray(a)
+    if dtype == torch.float32 and arr.dtype == np.float64:
+        # upload as is and round on the device (the same IEEE round-to-nearest as numpy's astype)
+        return torch.from_numpy(arr).to(dev).to(torch.float32)
     if dtype == torch.uint8:
         arr = arr.astype(np.uint8, copy=False)
     elif dtype == torch.float32:

@@ -85,8 +85,22 @@ class CoupledAblationEngine:
         self.mc_engine, self.thermal_engine = mc_engine, thermal_engine
         self.use_gpu_thermal = True
 
-        # ---- host set-up in float64, exactly as coupled_ablation.py:232-303 ----
-        optical = {key: np.array(optical_props[key], dtype=np.float64, copy=True) for key in ('mu_a', 'mu_s', 'g', 'n')}
+        # ---- set-up in float64, exactly as coupled_ablation.py:232-303, but on the device: the
+        # inputs are uploaded once and every step (stability clamp, void properties, wet copies) is
+        # the same IEEE float64 arithmetic as the host version, rounded to float32 at the end ----
+        d = self.dev
+
+        def h64(a):
+            if isinstance(a, torch.Tensor):
+                return a.to(device=d, dtype=torch.float64).clone()
+            return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(d)
+
+        def hbool(a):
+            if isinstance(a, torch.Tensor):
+                return a.to(device=d).bool()
+            return torch.from_numpy(np.ascontiguousarray(a, dtype=np.bool_)).to(d)
+
+        optical = {key: h64(optical_props[key]) for key in ('mu_a', 'mu_s', 'g', 'n')}
         self.Nx, self.Ny, self.Nz = optical['mu_a'].shape
         self.shape = (self.Nx, self.Ny, self.Nz)
         self.Lx, self.Ly, self.Lz = float(Lx), float(Ly), float(Lz)
@@ -107,40 +121,36 @@ class CoupledAblationEngine:
         self.use_graphs = bool(use_graphs)
         self.seed = int(seed) if seed is not None else int(np.random.randint(1, 2 ** 31 - 1))
 
-        k = np.array(k_grid, dtype=np.float64, copy=True)
-        rho = np.array(rho_cp_grid, dtype=np.float64, copy=True)
-        h_lat = np.array(h_lat_grid, dtype=np.float64, copy=True)
+        k, rho, h_lat = h64(k_grid), h64(rho_cp_grid), h64(h_lat_grid)
         inv_d2 = 1.0 / self.dx ** 2 + 1.0 / self.dy ** 2 + 1.0 / self.dz ** 2
         self.alpha_max_stable = stability_factor / (self.dt_sub * inv_d2)
-        alpha = k / np.maximum(rho, 1e-12)
+        alpha = k / torch.clamp(rho, min=1e-12)
         unstable = alpha > self.alpha_max_stable
-        self.cfl_conditioned_mask = unstable.copy()
-        if np.any(unstable):
-            rho[unstable] = k[unstable] / self.alpha_max_stable
+        self._cfl_mask = unstable
+        rho = torch.where(unstable, k / self.alpha_max_stable, rho)
         self.k_void = float(k_void)
         self.rho_cp_void = max(float(rho_cp_void), self.k_void / self.alpha_max_stable)
 
-        T = np.full(self.shape, self.t_ambient)
-        ablation_time = np.full(self.shape, -1.0)
+        ablation_time = torch.full(self.shape, -1.0, device=d, dtype=torch.float32)
         if initial_ablated_mask is not None:
-            ablated = np.array(initial_ablated_mask, dtype=np.bool_, copy=True)
-            ablation_time[ablated] = 0.0
-            optical['mu_a'][ablated] = 0.0; optical['mu_s'][ablated] = 0.0
-            optical['g'][ablated] = 0.0; optical['n'][ablated] = 1.0
-            k[ablated] = self.k_void
-            rho[ablated] = self.rho_cp_void
-            T[ablated] = self.t_ambient
+            ablated = hbool(initial_ablated_mask).reshape(self.shape)
+            ablation_time.masked_fill_(ablated, 0.0)
+            for key, v in (('mu_a', 0.0), ('mu_s', 0.0), ('g', 0.0), ('n', 1.0)):
+                optical[key].masked_fill_(ablated, v)
+            k.masked_fill_(ablated, self.k_void)
+            rho.masked_fill_(ablated, self.rho_cp_void)
         else:
-            ablated = np.zeros(self.shape, dtype=np.bool_)
+            ablated = torch.zeros(self.shape, dtype=torch.bool, device=d)
         self.arrhenius = None if arrhenius is None else (float(arrhenius[0]), float(arrhenius[1]) / R_GAS)
-        dry = (np.array(initial_dry_mask, dtype=np.bool_, copy=True) if initial_dry_mask is not None
-               else np.zeros(self.shape, dtype=np.bool_))
+        dry = (hbool(initial_dry_mask).reshape(self.shape) if initial_dry_mask is not None
+               else torch.zeros(self.shape, dtype=torch.bool, device=d))
         self.dry_state = dict(dry_state) if dry_state is not None else None
         wet = None
         if self.dry_state is not None:
-            if isinstance(self.dry_state.get('rho_cp'), np.ndarray):
-                self.dry_state['rho_cp'] = np.maximum(self.dry_state['rho_cp'], k / self.alpha_max_stable)
-            wet = (optical['mu_a'].copy(), k.copy(), rho.copy())
+            rc = self.dry_state.get('rho_cp')
+            if isinstance(rc, (np.ndarray, torch.Tensor)):
+                self.dry_state['rho_cp'] = torch.maximum(h64(rc), k / self.alpha_max_stable)
+            wet = (optical['mu_a'], k, rho)
         self.t_void = float(np.max(self.dry_state['t_remove'])) if self.dry_state is not None else self.t_abl
         self.char_state = char_state
         if char_state is not None:
@@ -152,26 +162,26 @@ class CoupledAblationEngine:
         self.air_gap_range = tuple(air_gap_range) if air_gap_range is not None else None
         self.wavelength_nm = float(wavelength_nm)
 
-        # ---- device fields ----
-        d = self.dev
-        f32 = lambda a: to_dev(a, d).reshape(self.shape)
+        # ---- device fields (float32) ----
+        f32 = lambda t: t.to(torch.float32).reshape(self.shape).contiguous()
         z32 = lambda: torch.zeros(self.shape, device=d, dtype=torch.float32)
         self._opt_t = {key: f32(optical[key]) for key in ('mu_a', 'mu_s', 'g', 'n')}
         self._k, self._rho, self._h_lat = f32(k), f32(rho), f32(h_lat)
-        self._T, self._T_alt = f32(T), z32()
+        self._T = torch.full(self.shape, self.t_ambient, device=d, dtype=torch.float32)
+        self._T_alt = z32()
         self._H = z32()
         self._Omega = z32()
         self._chi = z32()
         self._T_peak = torch.full(self.shape, self.t_ambient, device=d, dtype=torch.float32)
-        self._abl_time = f32(ablation_time)
-        flags = ablated.astype(np.uint8) * _lib.FLAG_ABLATED | dry.astype(np.uint8) * _lib.FLAG_DRY
-        self._flags = to_dev(flags, d, torch.uint8).reshape(self.shape)
+        self._abl_time = ablation_time
+        self._flags = (ablated.to(torch.uint8) * _lib.FLAG_ABLATED) | (dry.to(torch.uint8) * _lib.FLAG_DRY)
         self._wet = tuple(f32(w) for w in wet) if wet is not None else None
         self._A = z32()
         self._L = z32() if self.tally_fluence else None
         self._props = torch.zeros(self.Nx * self.Ny * self.Nz * 4, device=d, dtype=torch.float32)
         self._latz = torch.zeros(self.Nz, device=d, dtype=torch.float64)
         self._keep = []
+        del optical, k, rho, h_lat, alpha
 
         # plume (diffusion model, point injection)
         self.plume_closure = plume_closure
@@ -198,11 +208,19 @@ class CoupledAblationEngine:
         self.last_mc = None
         self._last_power = 0.0
 
+    @property
+    def cfl_conditioned_mask(self) -> np.ndarray:
+        """Voxels whose rho_cp was raised to keep the explicit step stable (coupled_ablation.py:246-250)."""
+        return self._cfl_mask.cpu().numpy()
+
     # ------------------------------------------------------------------------------
     def _gref(self, v):
         if v is None:
             return _lib.GridRef(None, 0.0, 0)
-        if np.ndim(v) == 0 or np.size(v) == 1:
+        if isinstance(v, torch.Tensor):
+            if v.numel() == 1:
+                return _lib.GridRef(None, float(v.reshape(-1)[0]), 0)
+        elif np.ndim(v) == 0 or np.size(v) == 1:
             return _lib.GridRef(None, float(np.asarray(v).ravel()[0]), 0)
         t = to_dev(v, self.dev).reshape(-1)
         self._keep.append(t)
