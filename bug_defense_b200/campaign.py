@@ -83,11 +83,13 @@ def campaign_instances(seed: int = 0, wavelengths=WAVELENGTHS_NM, powers=POWERS_
     return out
 
 
-def instance_geometry(inst: dict) -> dict:
-    """full_coupled_run geometry of an instance with its optics moved from 532 nm to its wavelength."""
+def instance_geometry(inst: dict, device=None) -> dict:
+    """full_coupled_run geometry of an instance with its optics moved from 532 nm to its wavelength;
+    with `device` the grids are built there (torch float64) and never exist on the host."""
     from . import workloads
     nx, ny, nz = inst["grid"]
-    geo = workloads.full_coupled_run(inst["tissue_seed"], nx=nx, ny=ny, nz=nz, n_plume_air=inst["n_plume_air"])
+    geo = workloads.full_coupled_run(inst["tissue_seed"], nx=nx, ny=ny, nz=nz, n_plume_air=inst["n_plume_air"],
+                                     device=device)
     nm = inst["wavelength_nm"]
     rng = np.random.default_rng(inst["mix_seed"])
     names = geo["layer_names"]
@@ -104,6 +106,10 @@ def instance_geometry(inst: dict) -> dict:
             m = mixes[name]
             scale_a[kk] = mix_mua(m, nm) / mix_mua(m, 532.0)
             scale_s[kk] = (nm / 532.0) ** -m["b_mie"]
+    if device is not None:
+        import torch
+        scale_a = torch.as_tensor(scale_a, device=torch.device(device))
+        scale_s = torch.as_tensor(scale_s, device=torch.device(device))
     for key, sc in (("mu_a", scale_a), ("mu_s", scale_s)):
         geo["optical"][key] = geo["optical"][key] * sc[None, None, :]
         geo["dry_state"][key] = geo["dry_state"][key] * sc[None, None, :]
@@ -121,7 +127,9 @@ def instance_geometry(inst: dict) -> dict:
 def make_engine(inst: dict, device=None, use_graphs: bool = True):
     from .coupled import CoupledAblationEngine
     from .workloads import engine_kwargs
-    geo = instance_geometry(inst)
+    import torch
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    geo = instance_geometry(inst, device=dev)
     kw = engine_kwargs(geo)
     kw.update(wavelength_nm=geo["wavelength_nm"], power=geo["power"], use_graphs=use_graphs, device=device,
               tally_fluence=False)

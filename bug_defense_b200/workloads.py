@@ -70,7 +70,7 @@ def single_epoch_stack(seed: int = 0, nx: int = 64, ny: int = 64, nz: int = 128)
         power=40.0, spot_dia=0.5, theta_inc_deg=22.0, n_photons=20_000, n_substeps=20, dt_sub=5e-5, seed=seed)
 
 
-def full_coupled_run(seed: int = 0, nx: int = 200, ny: int = 200, nz: int = 128, n_plume_air: int = 64):
+def full_coupled_run(seed: int = 0, nx: int = 200, ny: int = 200, nz: int = 128, n_plume_air: int = 64, device=None):
     """200x200x128 stack with 64 air slices prepended for the plume (200x200x192), boiling at 100 C with
     2.26 MJ/kg x water fraction, cuticle dry with removal at 350 C, char A ~ U(1e10, 1e12)/s,
     Ea ~ U(1.5e5, 2e5) J/mol, plume D ~ U(10, 50) mm^2/s, extinction ~ U(0.5, 5)/mm per unit
@@ -79,7 +79,7 @@ def full_coupled_run(seed: int = 0, nx: int = 200, ny: int = 200, nz: int = 128,
     lay = _draw_layers(rng)
     n_tissue = int(round(sum(t for _, t in STACK) * 1e-3 / DX))
     n_air = nz - n_tissue + n_plume_air
-    geo = _build(lay, nx, ny, n_air, n_tissue, wet_ablation=True)
+    geo = _build(lay, nx, ny, n_air, n_tissue, wet_ablation=True, device=device)
     char_A = float(rng.uniform(1e10, 1e12))
     char_Ea = float(rng.uniform(1.5e5, 2.0e5))
     D = float(rng.uniform(10.0, 50.0))
@@ -95,39 +95,48 @@ def full_coupled_run(seed: int = 0, nx: int = 200, ny: int = 200, nz: int = 128,
     return geo
 
 
-def _build(lay, nx, ny, n_air, n_tissue, wet_ablation):
+def _build(lay, nx, ny, n_air, n_tissue, wet_ablation, device=None):
+    """Layer properties per z slice, expanded to full (nx, ny, nz) grids: float64 numpy arrays, or
+    float64 torch tensors built on `device` (the per-instance builder of a campaign, no host grids)."""
     nz = n_air + n_tissue
     names = _layer_index(n_tissue, n_air)
     shape = (nx, ny, nz)
-    f = lambda v: np.full(shape, v, dtype=np.float64)
-    mu_a, mu_s, g, n = f(0.0), f(0.0), f(0.0), f(1.0)
-    k, rho_cp, h_lat = f(0.026e-3), f(1.206e-6), f(1e12)
-    dry = np.zeros(shape, bool)
-    ablated = np.zeros(shape, bool)
+    col = {key: np.full(nz, v, dtype=np.float64) for key, v in (("mu_a", 0.0), ("mu_s", 0.0), ("g", 0.0), ("n", 1.0),
+                                                                ("k", 0.026e-3), ("rho_cp", 1.206e-6),
+                                                                ("h_lat", 1e12))}
+    dry_z = np.zeros(nz, bool)
+    abl_z = np.zeros(nz, bool)
     gap = [kk for kk, nm in enumerate(names) if nm == "air_gap"]
     for kk, nm in enumerate(names):
         if nm == "top_air":
-            ablated[:, :, kk] = True
+            abl_z[kk] = True
             continue
         if nm == "below":
             continue
         p = lay[nm]
-        mu_a[:, :, kk] = p["mu_a"]; mu_s[:, :, kk] = p["mu_s"]; g[:, :, kk] = p["g"]; n[:, :, kk] = p["n"]
-        k[:, :, kk] = p["k"]; rho_cp[:, :, kk] = p["rho_cp"]
+        for key in ("mu_a", "mu_s", "g", "n", "k", "rho_cp"):
+            col[key][kk] = p[key]
         if nm == "air_gap":
             continue
         if "cuticle" in nm:
-            dry[:, :, kk] = wet_ablation
-            h_lat[:, :, kk] = 0.0 if wet_ablation else 1e12
+            dry_z[kk] = wet_ablation
+            col["h_lat"][kk] = 0.0 if wet_ablation else 1e12
         elif wet_ablation:
-            h_lat[:, :, kk] = H_LAT_WATER_J_PER_KG * p["rho"] * p["water"] * 1e-9
+            col["h_lat"][kk] = H_LAT_WATER_J_PER_KG * p["rho"] * p["water"] * 1e-9
+    if device is None:
+        grid = lambda c: np.broadcast_to(c, shape).copy()
+    else:
+        import torch
+        dev = torch.device(device)
+        grid = lambda c: torch.as_tensor(c, device=dev).expand(shape).contiguous()
+    optical = {key: grid(col[key]) for key in ("mu_a", "mu_s", "g", "n")}
+    k, rho_cp, h_lat = grid(col["k"]), grid(col["rho_cp"]), grid(col["h_lat"])
     Lx, Ly, Lz = nx * DX, ny * DX, nz * DX
-    optical = dict(mu_a=mu_a, mu_s=mu_s, g=g, n=n)
     return dict(shape=shape, Lx=Lx, Ly=Ly, Lz=Lz, optical=optical, k_grid=k, rho_cp_grid=rho_cp, h_lat_grid=h_lat,
-                dry_mask=dry, ablated_mask=ablated, air_gap_range=(gap[0], gap[-1] + 1) if gap else None,
+                dry_mask=grid(dry_z), ablated_mask=grid(abl_z), air_gap_range=(gap[0], gap[-1] + 1) if gap else None,
                 layers=lay, layer_names=names, n_air_top=n_air,
-                dry_state=dict(mu_a=mu_a.copy(), mu_s=mu_s.copy(), g=g.copy(), n=n.copy(), k=k.copy(),
-                               rho_cp=rho_cp.copy(), t_remove=350.0))
+                dry_state=dict(**{key: grid(col[key]) for key in ("mu_a", "mu_s", "g", "n", "k", "rho_cp")},
+                               t_remove=350.0))
 
 
 def engine_kwargs(geo: dict) -> dict:
