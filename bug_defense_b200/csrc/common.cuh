@@ -24,7 +24,15 @@ constexpr float kTallyScale = 68719476736.0f;          // 2^36
 constexpr long long kTallyMaxPhotons = 1LL << 26;
 // Plume neighbourhood mask: one byte per voxel, z rows padded to a 16-byte pitch (TMA rows).
 inline int plume_mask_pitch(int nz) { return (nz + 15) / 16 * 16; }
-inline size_t plume_mask_bytes(int nx, int ny, int nz) { return (size_t)nx * ny * plume_mask_pitch(nz); }
+// After the mask bytes (rounded to 256): the void x-extent of every (z tile, y tile) column of
+// the persistent plume kernel, xmin[kPlumeMaxCols] | xmax[kPlumeMaxCols] | prefix[kPlumeMaxCols + 1].
+constexpr int kPlumeMaxCols = 1024;
+inline size_t plume_mask_only_bytes(int nx, int ny, int nz) {
+    return ((size_t)nx * ny * plume_mask_pitch(nz) + 255) / 256 * 256;
+}
+inline size_t plume_mask_bytes(int nx, int ny, int nz) {
+    return plume_mask_only_bytes(nx, ny, nz) + sizeof(int) * (3 * kPlumeMaxCols + 1);
+}
 
 // Launch-shape knobs (BD_TUNE_*) and the generation counter bumped by every change.
 int tune_value(int knob);

@@ -505,12 +505,99 @@ struct PlumeXM {
 struct PlumeRun {
     int n_kt, by, nx;  // z tiles, y stride of the tiles, x planes per column
     long long s0, s1;
+    // compacted sequence (k_plume_xm): column c contributes only its planes x0[c] .. x0[c] + len - 1
+    // that hold void voxels, at positions pre[c] .. pre[c+1] - 1; nullptr: every column, nx planes
+    const int* pre = nullptr;
+    const int* x0 = nullptr;
+    int n_cols = 0;
     __device__ __forceinline__ int4 segment(long long pos) const {
-        const int col = (int)(pos / nx), ib = (int)(pos - (long long)col * nx);
-        const int ie = (int)min((long long)nx, ib + (s1 - pos));
-        return make_int4((col % n_kt) * PL_BZ, (col / n_kt) * by, ib, ie);
+        if (pre == nullptr) {
+            const int col = (int)(pos / nx), ib = (int)(pos - (long long)col * nx);
+            const int ie = (int)min((long long)nx, ib + (s1 - pos));
+            return make_int4((col % n_kt) * PL_BZ, (col / n_kt) * by, ib, ie);
+        }
+        int lo = 0, hi = n_cols - 1;  // the last column starting at or before pos (skips empty ones)
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (pre[mid] <= pos) lo = mid; else hi = mid - 1;
+        }
+        const int ib = x0[lo] + (int)(pos - pre[lo]);
+        const int ie = (int)min((long long)(x0[lo] + pre[lo + 1] - pre[lo]), ib + (s1 - pos));
+        return make_int4((lo % n_kt) * PL_BZ, (lo / n_kt) * by, ib, ie);
     }
 };
+
+// Void x-extent of every (z tile, y tile) column of k_plume_xm, from this stage's mask (voxels at
+// or below the void limit are not void). ext = xmin | xmax | prefix, see plume_mask_bytes.
+__global__ void k_plume_extent_init(int* __restrict__ ext) {
+    for (int i = threadIdx.x; i < kPlumeMaxCols; i += blockDim.x) {
+        ext[i] = INT_MAX;
+        ext[kPlumeMaxCols + i] = -1;
+    }
+}
+
+// block (x, y tile): which z tiles of the plane tile hold a void voxel
+__global__ void __launch_bounds__(256) k_plume_extent(const uint8_t* __restrict__ M, int nx, int ny, int nz, int mz,
+                                                      const int* __restrict__ zlimit, int* __restrict__ ext) {
+    __shared__ unsigned long long s_bits;
+    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
+    const int n_kt = (zl + PL_BZ - 1) / PL_BZ;
+    const int x = blockIdx.x, jt = blockIdx.y;
+    if (threadIdx.x == 0) s_bits = 0ull;
+    __syncthreads();
+    unsigned long long bits = 0ull;
+    for (int i = threadIdx.x; i < PX_BY * zl; i += blockDim.x) {
+        const int r = i / zl, z = i - r * zl, j = jt * PX_BY + r;
+        if (j < ny && (M[((size_t)x * ny + j) * mz + z] & BD_PM_VOID)) bits |= 1ull << (z / PL_BZ);
+    }
+    if (bits) atomicOr(&s_bits, bits);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int kt = 0; kt < n_kt; ++kt)
+            if (s_bits & (1ull << kt)) {
+                atomicMin(&ext[jt * n_kt + kt], x);
+                atomicMax(&ext[kPlumeMaxCols + jt * n_kt + kt], x);
+            }
+    }
+}
+
+// one CTA: column lengths -> exclusive prefix (prefix[n_cols] = all planes); empty columns get x0 = 0
+__global__ void __launch_bounds__(1024) k_plume_runs(int* __restrict__ ext, int ny, int nz,
+                                                     const int* __restrict__ zlimit) {
+    __shared__ int wsum[32];
+    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
+    const int n_cols = ((zl + PL_BZ - 1) / PL_BZ) * ((ny + PX_BY - 1) / PX_BY);
+    const int c = threadIdx.x, lane = c & 31, warp = c >> 5;
+    int len = 0;
+    if (c < n_cols) {
+        const int lo = ext[c], hi = ext[kPlumeMaxCols + c];
+        len = hi >= lo ? hi - lo + 1 : 0;
+        if (len == 0) ext[c] = 0;
+    }
+    int incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int w = wsum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += u;
+        }
+        wsum[lane] = w;
+    }
+    __syncthreads();
+    const int before = (warp > 0 ? wsum[warp - 1] : 0) + incl - len;
+    int* pre = ext + 2 * kPlumeMaxCols;
+    if (c < n_cols) pre[c] = before;
+    if (c == n_cols - 1) pre[n_cols] = before + len;
+    if (n_cols == 0 && c == 0) pre[0] = 0;
+}
 
 // Every lane waits for the copy of load q; the vote keeps a timeout warp-uniform.
 __device__ __forceinline__ bool px_wait(unsigned long long* full, int q, volatile int* fail) {
@@ -557,18 +644,35 @@ template <int PB>
 __global__ void __launch_bounds__(PX_THREADS, 1) k_plume_xm(const __grid_constant__ CUtensorMap c_map,
                                                          const __grid_constant__ CUtensorMap m_map,
                                                          float* __restrict__ Cn, int nx, int ny, int nz, PlumeConst c,
-                                                         const int* __restrict__ zlimit, int full_write,
+                                                         const int* __restrict__ zlimit,
+                                                         const int* __restrict__ ext, int full_write,
                                                          int* __restrict__ err) {
     using X = PlumeXM<PB>;
     extern __shared__ __align__(128) unsigned char ring[];
     __shared__ __align__(8) unsigned long long full[PX_STAGES], empty[PX_STAGES];
     __shared__ volatile int s_fail;
+    __shared__ int s_x0[kPlumeMaxCols], s_pre[kPlumeMaxCols + 1];
     const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
     const int n_kt = (zl + PL_BZ - 1) / PL_BZ;
-    const long long total = (long long)n_kt * ((ny + PX_BY - 1) / PX_BY) * nx;
-    const PlumeRun run{n_kt, PX_BY, nx, total * blockIdx.x / gridDim.x, total * (blockIdx.x + 1) / gridDim.x};
-    if (run.s0 >= run.s1) return;  // uniform over the CTA
+    const int n_cols = n_kt * ((ny + PX_BY - 1) / PX_BY);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    long long total = (long long)n_cols * nx;
+    PlumeRun run{n_kt, PX_BY, nx, 0, 0};
+    if (ext) {
+        // only the planes of each column that hold void voxels (k_plume_extent / k_plume_runs)
+        for (int i = tid; i <= n_cols; i += blockDim.x) {
+            s_pre[i] = ext[2 * kPlumeMaxCols + i];
+            if (i < n_cols) s_x0[i] = ext[i];
+        }
+        __syncthreads();
+        total = s_pre[n_cols];
+        run.pre = s_pre;
+        run.x0 = s_x0;
+        run.n_cols = n_cols;
+    }
+    run.s0 = total * blockIdx.x / gridDim.x;
+    run.s1 = total * (blockIdx.x + 1) / gridDim.x;
+    if (run.s0 >= run.s1) return;  // uniform over the CTA
     if (tid == 0) {
         for (int q = 0; q < PX_STAGES; ++q) {
             mbar_init(&full[q], 1);
@@ -1122,6 +1226,7 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     const dim3 tgrid((p->nz + PL_BZ - 1) / PL_BZ, (p->ny + PL_BY - 1) / PL_BY, (p->nx + xc - 1) / xc);
     // persistent kernels: xc CTAs per SM (capped by occupancy), at most one per plane tile of the grid
     int xm_grid = 0, tb_grid = 0;
+    int* xm_ext = nullptr;
     unsigned xm_smem = shape == 1 ? PlumeXM<2>::SMEM : PlumeXM<4>::SMEM;
     if (tma && shape > 0) {
         int dev = 0, sms = 0, occ = 0;
@@ -1137,6 +1242,17 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
         const long long planes =
             (long long)((p->nz + PL_BZ - 1) / PL_BZ) * ((p->ny + PX_BY - 1) / PX_BY) * p->nx;
         xm_grid = (int)std::max(1LL, std::min(planes, (long long)std::max(std::min(occ, xc), 1) * sms));
+        // the void x-extent of every column, from this stage's mask: the persistent kernel walks
+        // only planes that hold void voxels (the void domain is fixed within the stage)
+        const int n_ktmax = (p->nz + PL_BZ - 1) / PL_BZ, n_jt = (p->ny + PX_BY - 1) / PX_BY;
+        if (n_ktmax <= 64 && n_ktmax * n_jt <= kPlumeMaxCols) {
+            xm_ext = reinterpret_cast<int*>(mask + plume_mask_only_bytes(p->nx, p->ny, p->nz));
+            k_plume_extent_init<<<1, 1024, 0, st>>>(xm_ext);
+            k_plume_extent<<<dim3(p->nx, n_jt), 256, 0, st>>>(mask, p->nx, p->ny, p->nz, mz,
+                                                              full_first ? nullptr : zlimit, xm_ext);
+            k_plume_runs<<<1, 1024, 0, st>>>(xm_ext, p->ny, p->nz, full_first ? nullptr : zlimit);
+            BD_CHECK_LAUNCH("k_plume_runs");
+        }
         if (two) {
             int occ2 = 0;
             BD_CUDA(cudaFuncSetAttribute(k_plume_tb<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1165,9 +1281,11 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
         }
         ++s;
         if (tma && shape == 1)
-            k_plume_xm<2><<<xm_grid, PX_THREADS, xm_smem, st>>>(map, map_m, out, p->nx, p->ny, p->nz, c, zl, full, err);
+            k_plume_xm<2><<<xm_grid, PX_THREADS, xm_smem, st>>>(map, map_m, out, p->nx, p->ny, p->nz, c, zl,
+                                                                full ? nullptr : xm_ext, full, err);
         else if (tma && shape == 2)
-            k_plume_xm<4><<<xm_grid, PX_THREADS, xm_smem, st>>>(map, map_m, out, p->nx, p->ny, p->nz, c, zl, full, err);
+            k_plume_xm<4><<<xm_grid, PX_THREADS, xm_smem, st>>>(map, map_m, out, p->nx, p->ny, p->nz, c, zl,
+                                                                full ? nullptr : xm_ext, full, err);
         else if (tma)
             k_plume_step_tma<<<tgrid, dim3(TZ, PL_TY), 0, st>>>(map, out, mask, p->nx, p->ny, p->nz, mz, xc, c, zl,
                                                              full, err);

@@ -73,7 +73,10 @@ def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
     slab = np.zeros((12, 70, 96), bool)                 # bulk void above z = 50, scattered pores below
     slab[:, :, :50] = True
     slab |= rng.uniform(size=slab.shape) < 0.1
-    for vd in (scattered, slab):
+    cavity = np.zeros((12, 70, 132), bool)              # deep z tiles void only in a small cavity, the
+    cavity[:, :, :40] = True                            # deepest none: trimmed and empty columns
+    cavity[3:7, 20:41, 70:101] = True
+    for vd in (scattered, slab, cavity):
         shape = vd.shape
         C0 = (rng.uniform(0, 1, shape) * vd).astype(np.float32)
         z = np.zeros(shape)
