@@ -155,12 +155,29 @@ def _stage_ms(eng, n_epochs: int, laser: bool) -> np.ndarray:
     return np.array(ms[:]) / max(int(n.value), 1)
 
 
+def _epoch_ms(eng, n_epochs: int, laser: bool) -> float:
+    """Whole-epoch time (ms, device events) over n_epochs: with the plume stage beside MC and the
+    substeps, a stage's span is not what a launch shape should minimise."""
+    import torch
+    eng.power = eng.laser_power if laser else 0.0
+    st = torch.cuda.current_stream(eng.dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(n_epochs):
+        eng._enqueue(0)
+    e1.record(st)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / max(n_epochs, 1)
+
+
 def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=None) -> dict:
     """Pick launch shapes by timing them on a throwaway engine of the real workload: `inst` is a
     campaign instance dict or a callable returning an engine with a `laser_power` attribute.
-    Tries MC CTAs per SM (photons per thread) on laser-on epochs, x-planes per CTA of the fused
-    substep kernel, the plume kernel and its x-planes (kernel 0) or CTAs per SM (kernel 1); sets the winning values process-wide (bd_tune_set) and
-    returns the choices with every trial's per-epoch stage time (ms)."""
+    MC CTAs per SM (photons per thread) are timed by the MC stage of laser-on epochs; x-planes per
+    CTA of the fused substep kernel, the plume kernel and its x-planes (kernel 0) or CTAs per SM
+    (persistent kernels) by the whole epoch with the laser off, when the void domain does not
+    change between trials. Sets the winning values process-wide (bd_tune_set) and returns the
+    choices with every trial's time (ms per epoch)."""
     from . import _lib
     cand = dict(candidates or {})
     cand.setdefault(_lib.TUNE_MC_BLOCKS_PER_SM, [2, 4, 6, 8])
@@ -175,13 +192,15 @@ def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=
     out = {"trials": {}}
     for knob, values in cand.items():
         trials = []
+        mc = knob == _lib.TUNE_MC_BLOCKS_PER_SM
         for v in values:
             _lib.call("bd_tune_set", int(knob), int(v))
-            _stage_ms(eng, 1, laser=True)    # re-capture the stage graphs for the new shape
-            ms = _stage_ms(eng, epochs_per_trial, laser=True)
-            trials.append((int(v), float(ms[stage[knob]])))
+            _stage_ms(eng, 1, laser=mc)      # re-capture the stage graphs for the new shape
+            t = (float(_stage_ms(eng, epochs_per_trial, laser=True)[stage[knob]]) if mc
+                 else _epoch_ms(eng, epochs_per_trial, laser=False))
+            trials.append((int(v), t))
             if log:
-                log(f"autotune {names[knob]}={v}: {ms[stage[knob]]:.3f} ms/epoch")
+                log(f"autotune {names[knob]}={v}: {t:.3f} ms/epoch")
         best = min(trials, key=lambda t: t[1])[0]
         _lib.call("bd_tune_set", int(knob), int(best))
         out[names[knob]] = best
