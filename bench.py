@@ -214,12 +214,12 @@ def run_ours(args, rank, world, local):
 
 def e2e_run(args, geo, dev, K):
     """Same metric through the public API from host arrays: engine construction (upload of every
-    field from host numpy), K epochs each returning the diagnostics dict and pulling the runner's
-    per-epoch recording (xz slices of T, Q, phase and plume at mid-y: run_highres_knowledge_suite.py:280-306)."""
+    field from host numpy), K epochs each returning the diagnostics dict, and the runner's per-epoch
+    recording (xz slices of T, Q, phase and plume at mid-y, run_highres_knowledge_suite.py:280-306)
+    through Recorder into pinned host memory."""
     import numpy as np
     import torch
-    from bug_defense_b200 import workloads
-    from bug_defense_b200.phase import compute_phase_map
+    from bug_defense_b200.record import Recorder
     torch.cuda.synchronize()
     st = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -229,25 +229,17 @@ def e2e_run(args, geo, dev, K):
                                                geo["optical"]["n"], geo["k_grid"], geo["rho_cp_grid"],
                                                geo["h_lat_grid"], geo["dry_mask"], geo["ablated_mask"]))
     h2d += sum(np.asarray(geo["dry_state"][k]).nbytes for k in ("mu_a", "mu_s", "g", "n", "k", "rho_cp"))
-    my = eng.Ny // 2
     n_on = max(1, int(round(LASER_DUTY * K)))
-    pinned = {k: torch.empty((eng.Nx, eng.Nz), dtype=dt, pin_memory=True)
-              for k, dt in (("T", torch.float32), ("Q", torch.float32), ("phase", torch.uint8), ("plume", torch.float32))}
-    d2h = 0
-    scale = POWER_W / (eng.n_photons * eng.voxel_vol)
+    # the runner's per-epoch recording through the public Recorder: the device record kernel fills
+    # a slot (xz slices of T, Q, phase and plume at mid-y, depth, band peaks) that is copied into a
+    # pinned ring without a per-epoch synchronisation; step_epoch() returns the diagnostics dict
+    rec = Recorder(eng, k_surface=geo["n_air_top"], ring=16)
     for s in range(K):
         eng.power = POWER_W if s < n_on else 0.0
-        diag = eng.step_epoch()
-        flags = eng._flags[:, my, :]
-        ph = compute_phase_map(eng._T[:, my, :], eng._chi[:, my, :], (flags & 2) != 0, (flags & 1) != 0,
-                               eng._H[:, my, :])
-        pinned["T"].copy_(eng._T[:, my, :], non_blocking=True)
-        pinned["Q"].copy_(eng._A[:, my, :] * (scale if eng.power > 0 else 0.0), non_blocking=True)
-        pinned["phase"].copy_(ph, non_blocking=True)
-        pinned["plume"].copy_(eng.plume.raw[:, my, :], non_blocking=True)
-        torch.cuda.current_stream().synchronize()
-        d2h = ctypes.sizeof(__import__("bug_defense_b200")._lib.EpochDiag) + sum(
-            t.numel() * t.element_size() for t in pinned.values())
+        eng.step_epoch()
+        rec.record()
+    rec.finish()
+    d2h = ctypes.sizeof(__import__("bug_defense_b200")._lib.EpochDiag) + rec.slot_bytes
     e1.record(st)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
