@@ -279,7 +279,7 @@ def ours_main(args):
     kv = ctypes.c_int(0)
     _lib.call("bd_tune_get", _lib.TUNE_PLUME_KERNEL, ctypes.byref(kv))
     plume_kernel = {0: "k_plume_step_tma", 1: "k_plume_xm<2>", 2: "k_plume_xm<4>",
-                    3: "k_plume_tb<2>"}.get(kv.value, "k_plume_step")
+                    3: "k_plume_tb<2>", 4: "k_plume_direct"}.get(kv.value, "k_plume_step")
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():

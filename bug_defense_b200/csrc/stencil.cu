@@ -640,6 +640,87 @@ __device__ __forceinline__ bool all_interior(unsigned m) {
     return (m & (upd * 0x3Fu)) == upd * 0x3Fu;
 }
 
+// Direct plume step: no staging, no barriers. A CTA is one 32 (z) x 32 (y) tile and marches xc x
+// planes; thread = 4 consecutive z voxels of one row, a warp 8 such groups x 4 rows (one 128-byte
+// line per row and load). The thread keeps the x-1 / x / x+1 float4 of its row in registers and
+// loads, per plane, the next plane's float4 and the centre plane's y neighbours from the
+// (L2-resident) field; the z neighbours come from the neighbouring lanes by shuffle (the tile's
+// edge lanes load them), the mask bytes as one 32-bit load. Latency is hidden by the many
+// independent CTAs of a step instead of a copy pipeline. Warp-uniform paths as in k_plume_xm;
+// the same per-voxel expression (bit-identical). Needs nz % 4 == 0 and 16-byte aligned fields.
+__global__ void __launch_bounds__(256) k_plume_direct(const float* __restrict__ C, float* __restrict__ Cn,
+                                                      const uint8_t* __restrict__ M, int nx, int ny, int nz, int mz,
+                                                      int xc, PlumeConst c, const int* __restrict__ zlimit,
+                                                      int full_write) {
+    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
+    const int k0 = blockIdx.x * PL_BZ;
+    const int ib = blockIdx.z * xc, ie = min(nx, ib + xc);
+    if (k0 >= zl || ib >= ie) return;  // uniform over the CTA
+    const int zg = threadIdx.x & 7;
+    const int j = blockIdx.y * PX_BY + (threadIdx.x >> 3), k = k0 + 4 * zg;
+    const int nk = zl - k;
+    const bool act = nk > 0 && j < ny;
+    const bool in = j < ny && k < nz;
+    const unsigned zkeep = nk >= 4 ? 0xffffffffu : (nk <= 0 ? 0u : (0xffffffffu >> (8 * (4 - nk))));
+    const size_t plane = (size_t)ny * nz;
+    const size_t mplane = (size_t)ny * mz;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    size_t idx = ((size_t)ib * ny + j) * nz + k;
+    const uint8_t* mp = M + ((size_t)ib * ny + j) * mz + k;
+    PlumeW kw;
+    kw.wx = c.dtp * c.dxy_x; kw.wy = c.dtp * c.dxy_y; kw.wb = c.dtp * c.dz_z;
+    kw.wt = kw.wb + c.dtp * c.vz_over_dz;
+    kw.w0 = 1.0f - 2.0f * (kw.wx + kw.wy + kw.wb) - c.dtp * c.vz_over_dz;
+    kw.decay = c.decay;
+    // cw / cc / ce: planes i-1 / i / i+1 of the row, loaded only for planes a warp computes (the
+    // flags are warp-uniform); a plane with nothing to write loads nothing but its mask bytes
+    float4 cw = z4, cc = z4, ce = z4;
+    bool hw = false, hc = false;
+    for (int i = ib; i < ie; ++i, idx += plane, mp += mplane) {
+        const unsigned mr = act ? (__ldg(reinterpret_cast<const unsigned*>(mp)) & zkeep) : 0u;
+        const unsigned vd = mr & 0x40404040u;
+        bool he = false;
+        if (__any_sync(0xffffffffu, act && (vd || full_write))) {
+            if (!hw) cw = in && i > 0 ? __ldg(reinterpret_cast<const float4*>(C + idx - plane)) : z4;
+            if (!hc) cc = in ? __ldg(reinterpret_cast<const float4*>(C + idx)) : z4;
+            ce = in && i + 1 < nx ? __ldg(reinterpret_cast<const float4*>(C + idx + plane)) : z4;
+            he = true;
+            const float4 cs = in && j > 0 ? __ldg(reinterpret_cast<const float4*>(C + idx - nz)) : z4;
+            const float4 cn = in && j + 1 < ny ? __ldg(reinterpret_cast<const float4*>(C + idx + nz)) : z4;
+            float zb = __shfl_up_sync(0xffffffffu, cc.w, 1, 8);
+            float zt = __shfl_down_sync(0xffffffffu, cc.x, 1, 8);
+            if (zg == 0) zb = in && k > 0 ? __ldg(C + idx - 1) : 0.0f;
+            if (zg == 7) zt = in && k + 4 < nz ? __ldg(C + idx + 4) : 0.0f;
+            float v[4];
+            if (__all_sync(0xffffffffu, all_interior(mr) || !act)) {
+                v[0] = ftcs<true>(cc.x, cw.x, ce.x, cs.x, cn.x, zb, cc.y, mr & 0xffu, kw);
+                v[1] = ftcs<true>(cc.y, cw.y, ce.y, cs.y, cn.y, cc.x, cc.z, (mr >> 8) & 0xffu, kw);
+                v[2] = ftcs<true>(cc.z, cw.z, ce.z, cs.z, cn.z, cc.y, cc.w, (mr >> 16) & 0xffu, kw);
+                v[3] = ftcs<true>(cc.w, cw.w, ce.w, cs.w, cn.w, cc.z, zt, mr >> 24, kw);
+            } else {
+                v[0] = ftcs<false>(cc.x, cw.x, ce.x, cs.x, cn.x, zb, cc.y, mr & 0xffu, kw);
+                v[1] = ftcs<false>(cc.y, cw.y, ce.y, cs.y, cn.y, cc.x, cc.z, (mr >> 8) & 0xffu, kw);
+                v[2] = ftcs<false>(cc.z, cw.z, ce.z, cs.z, cn.z, cc.y, cc.w, (mr >> 16) & 0xffu, kw);
+                v[3] = ftcs<false>(cc.w, cw.w, ce.w, cs.w, cn.w, cc.z, zt, mr >> 24, kw);
+            }
+            if (act && (vd || full_write)) {
+                float* dst = Cn + idx;
+                if (full_write || vd == 0x40404040u) {
+                    *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                        if (vd & (0x40u << (8 * e))) dst[e] = v[e];
+                }
+            }
+        }
+        cw = cc;
+        hw = hc;
+        cc = ce;
+        hc = he;
+    }
+}
+
 template <int PB>
 __global__ void __launch_bounds__(PX_THREADS, 1) k_plume_xm(const __grid_constant__ CUtensorMap c_map,
                                                          const __grid_constant__ CUtensorMap m_map,
@@ -1212,7 +1293,7 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     // 3 = two steps per launch (k_plume_tb, 2 planes per copy; single steps on kernel 1)
     // (64 registers x 288 threads: at most 3 CTAs per SM; 4 at 56 registers measured slower)
     const int kernel = tune_value(BD_TUNE_PLUME_KERNEL);
-    const int shape = kernel == 3 ? 1 : kernel;  // the one-step kernel
+    const int shape = kernel >= 3 ? 1 : kernel;  // the one-step kernel (kernel 4 launches its own)
     const int pb = shape == 1 ? 2 : 4;
     const int py = shape == 0 ? PL_PY : PX_PY;
     const int pz = shape == 0 ? PL_PZ : PX_PZ;
@@ -1273,6 +1354,12 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
         const CUtensorMap& map = odd ? map_b : map_a;
         const int* zl = full ? nullptr : zlimit;
         ++launches;
+        if (kernel == 4 && tma) {
+            ++s;
+            k_plume_direct<<<dim3((p->nz + PL_BZ - 1) / PL_BZ, (p->ny + PX_BY - 1) / PX_BY, (p->nx + xc - 1) / xc),
+                             256, 0, st>>>(in, out, mask, p->nx, p->ny, p->nz, mz, xc, c, zl, full);
+            continue;
+        }
         if (two && !full && total - s >= 2) {
             k_plume_tb<2><<<tb_grid, PX_THREADS, PlumeTB<2>::SMEM, st>>>(map, map_m2, out, p->nx, p->ny, p->nz, c, zl,
                                                                        err);

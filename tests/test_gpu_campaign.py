@@ -35,7 +35,7 @@ def test_knob_validation(gpu, restore_knobs):
     with pytest.raises(ValueError):
         _knob(_lib.TUNE_MC_BLOCKS_PER_SM, 17)
     with pytest.raises(ValueError):
-        _knob(_lib.TUNE_PLUME_KERNEL, 4)
+        _knob(_lib.TUNE_PLUME_KERNEL, 5)
     with pytest.raises(ValueError):
         _knob(7, 1)
 
@@ -81,7 +81,7 @@ def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
         C0 = (rng.uniform(0, 1, shape) * vd).astype(np.float32)
         z = np.zeros(shape)
         fields = []
-        for kern, xc in ((0, 4), (0, 2), (1, 4), (1, 1), (2, 2), (2, 1), (1, 3), (3, 2), (3, 1)):
+        for kern, xc in ((0, 4), (0, 2), (1, 4), (1, 1), (2, 2), (2, 1), (1, 3), (3, 2), (3, 1), (4, 2)):
             _knob(_lib.TUNE_PLUME_KERNEL, kern)
             _knob(_lib.TUNE_PLUME_XC, xc)
             ctx = gpu.MetalAblationContext(*shape, 0.03, 0.025, 0.02, 1e-5, 0.0, 20.0, 100.0, 300.0,
@@ -96,7 +96,7 @@ def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
         assert np.any(fields[0] != C0)
     inst = _small(22)                                  # 2940 nm, 80 W: a crater opens
     runs = []
-    for kern in (0, 1, 2, 3):
+    for kern in (0, 1, 2, 3, 4):
         _knob(_lib.TUNE_PLUME_KERNEL, kern)
         camp = campaign.Campaign([inst])
         camp.run(14, sync_every=14)
