@@ -183,7 +183,7 @@ def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=
     cand.setdefault(_lib.TUNE_MC_BLOCKS_PER_SM, [2, 4, 6, 8])
     cand.setdefault(_lib.TUNE_STENCIL_XC, [4, 8, 16])
     cand.setdefault(_lib.TUNE_PLUME_KERNEL, [0, 1, 2, 3, 4])
-    cand.setdefault(_lib.TUNE_PLUME_XC, [2, 4, 6, 8])
+    cand.setdefault(_lib.TUNE_PLUME_XC, [2, 3, 4, 6])
     stage = {_lib.TUNE_MC_BLOCKS_PER_SM: 0, _lib.TUNE_STENCIL_XC: 1, _lib.TUNE_PLUME_XC: 2, _lib.TUNE_PLUME_KERNEL: 2}
     names = {_lib.TUNE_MC_BLOCKS_PER_SM: "mc_ctas_per_sm", _lib.TUNE_STENCIL_XC: "stencil_xc",
              _lib.TUNE_PLUME_XC: "plume_xc", _lib.TUNE_PLUME_KERNEL: "plume_kernel"}

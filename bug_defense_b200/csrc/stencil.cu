@@ -640,15 +640,17 @@ __device__ __forceinline__ bool all_interior(unsigned m) {
     return (m & (upd * 0x3Fu)) == upd * 0x3Fu;
 }
 
-// Direct plume step: no staging, no barriers. A CTA is one 32 (z) x 32 (y) tile and marches xc x
+// Direct plume step: no staging, no barriers. A CTA is one 32 (z) x 16 (y) tile and marches xc x
 // planes; thread = 4 consecutive z voxels of one row, a warp 8 such groups x 4 rows (one 128-byte
-// line per row and load). The thread keeps the x-1 / x / x+1 float4 of its row in registers and
+// line per row and load). Smaller tiles measured faster than 32 or 64 rows (more CTAs to hide
+// latency with). The thread keeps the x-1 / x / x+1 float4 of its row in registers and
 // loads, per plane, the next plane's float4 and the centre plane's y neighbours from the
 // (L2-resident) field; the z neighbours come from the neighbouring lanes by shuffle (the tile's
 // edge lanes load them), the mask bytes as one 32-bit load. Latency is hidden by the many
 // independent CTAs of a step instead of a copy pipeline. Warp-uniform paths as in k_plume_xm;
 // the same per-voxel expression (bit-identical). Needs nz % 4 == 0 and 16-byte aligned fields.
-__global__ void __launch_bounds__(256) k_plume_direct(const float* __restrict__ C, float* __restrict__ Cn,
+constexpr int PD_BY = 16;  // rows per CTA (8 * PD_BY threads)
+__global__ void __launch_bounds__(8 * PD_BY) k_plume_direct(const float* __restrict__ C, float* __restrict__ Cn,
                                                       const uint8_t* __restrict__ M, int nx, int ny, int nz, int mz,
                                                       int xc, PlumeConst c, const int* __restrict__ zlimit,
                                                       int full_write) {
@@ -657,7 +659,7 @@ __global__ void __launch_bounds__(256) k_plume_direct(const float* __restrict__ 
     const int ib = blockIdx.z * xc, ie = min(nx, ib + xc);
     if (k0 >= zl || ib >= ie) return;  // uniform over the CTA
     const int zg = threadIdx.x & 7;
-    const int j = blockIdx.y * PX_BY + (threadIdx.x >> 3), k = k0 + 4 * zg;
+    const int j = blockIdx.y * PD_BY + (threadIdx.x >> 3), k = k0 + 4 * zg;
     const int nk = zl - k;
     const bool act = nk > 0 && j < ny;
     const bool in = j < ny && k < nz;
@@ -1356,8 +1358,8 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
         ++launches;
         if (kernel == 4 && tma) {
             ++s;
-            k_plume_direct<<<dim3((p->nz + PL_BZ - 1) / PL_BZ, (p->ny + PX_BY - 1) / PX_BY, (p->nx + xc - 1) / xc),
-                             256, 0, st>>>(in, out, mask, p->nx, p->ny, p->nz, mz, xc, c, zl, full);
+            k_plume_direct<<<dim3((p->nz + PL_BZ - 1) / PL_BZ, (p->ny + PD_BY - 1) / PD_BY, (p->nx + xc - 1) / xc),
+                             8 * PD_BY, 0, st>>>(in, out, mask, p->nx, p->ny, p->nz, mz, xc, c, zl, full);
             continue;
         }
         if (two && !full && total - s >= 2) {
