@@ -1311,7 +1311,7 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     int xm_grid = 0, tb_grid = 0;
     int* xm_ext = nullptr;
     unsigned xm_smem = shape == 1 ? PlumeXM<2>::SMEM : PlumeXM<4>::SMEM;
-    if (tma && shape > 0) {
+    if (tma && shape > 0 && kernel != 4) {
         int dev = 0, sms = 0, occ = 0;
         BD_CUDA(cudaGetDevice(&dev));
         BD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
