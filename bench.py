@@ -224,7 +224,11 @@ def e2e_run(args, geo, dev, K):
     st = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(st)
+    h0 = time.perf_counter()
     eng = make_engine(geo, dev, seed_offset=101)
+    h1 = time.perf_counter()
+    ec = torch.cuda.Event(enable_timing=True)
+    ec.record(st)
     h2d = sum(np.asarray(v).nbytes for v in (geo["optical"]["mu_a"], geo["optical"]["mu_s"], geo["optical"]["g"],
                                                geo["optical"]["n"], geo["k_grid"], geo["rho_cp_grid"],
                                                geo["h_lat_grid"], geo["dry_mask"], geo["ablated_mask"]))
@@ -244,7 +248,9 @@ def e2e_run(args, geo, dev, K):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     return {"value": K / (ms / 1e3), "unit": "epochs/s", "h2d_bytes_per_step": int(h2d / K),
-            "d2h_bytes_per_step": int(d2h), "note": "engine construction from host arrays + per-epoch diagnostics "
+            "d2h_bytes_per_step": int(d2h), "construct_ms": round(e0.elapsed_time(ec), 2),
+            "construct_host_ms": round((h1 - h0) * 1e3, 2),
+            "epochs_ms": round(ec.elapsed_time(e1), 2), "note": "engine construction from host arrays + per-epoch diagnostics "
                                                      "and xz recording slices, amortised over the timed epochs"}
 
 

@@ -207,6 +207,9 @@ class CoupledAblationEngine:
         self.epoch = 0
         self.last_mc = None
         self._last_power = 0.0
+        # host work that may run while the device finishes an enqueued epoch (weak references to
+        # bound methods, run by _diag just before it blocks on the epoch's diagnostics)
+        self._wait_hooks = []
 
     @property
     def cfl_conditioned_mask(self) -> np.ndarray:
@@ -410,7 +413,18 @@ class CoupledAblationEngine:
             self._enqueue(0)
         return self._diag(None)
 
+    def _run_wait_hooks(self):
+        live = []
+        for ref in self._wait_hooks:
+            fn = ref()
+            if fn is not None:
+                fn()
+                live.append(ref)
+        self._wait_hooks = live
+
     def _diag(self, absorbed_map):
+        if self._wait_hooks:
+            self._run_wait_hooks()
         dg = _lib.EpochDiag()
         _lib.call("bd_engine_read_diag", self._handle, ctypes.byref(dg), _lib.stream_ptr())
         self.t = dg.time_s

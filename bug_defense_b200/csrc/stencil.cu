@@ -642,13 +642,17 @@ __device__ __forceinline__ bool all_interior(unsigned m) {
 
 // Direct plume step: no staging, no barriers. A CTA is one 32 (z) x 16 (y) tile and marches xc x
 // planes; thread = 4 consecutive z voxels of one row, a warp 8 such groups x 4 rows (one 128-byte
-// line per row and load). Smaller tiles measured faster than 32 or 64 rows (more CTAs to hide
-// latency with). The thread keeps the x-1 / x / x+1 float4 of its row in registers and
-// loads, per plane, the next plane's float4 and the centre plane's y neighbours from the
-// (L2-resident) field; the z neighbours come from the neighbouring lanes by shuffle (the tile's
-// edge lanes load them), the mask bytes as one 32-bit load. Latency is hidden by the many
-// independent CTAs of a step instead of a copy pipeline. Warp-uniform paths as in k_plume_xm;
-// the same per-voxel expression (bit-identical). Needs nz % 4 == 0 and 16-byte aligned fields.
+// line per row and load). The thread keeps the x-1 / x float4 of its row in registers and loads,
+// per plane, the next plane's float4 and the centre plane's y neighbours from the (L2-resident)
+// field beside the plane's mask bytes (one 32-bit load), whether or not the warp then has void to
+// update: one L2 round trip per plane instead of a mask round trip followed by a data round trip,
+// at the price of loads a tissue plane does not need (L2 bandwidth has the headroom). The z
+// neighbours come from the neighbouring lanes by shuffle (the tile's edge lanes load them). Latency
+// is hidden by the many independent CTAs of a step instead of a copy pipeline. Warp-uniform paths
+// as in k_plume_xm; the same per-voxel expression (bit-identical). Needs nz % 4 == 0 and 16-byte
+// aligned fields. Measured on the full coupled run: 16-row tiles beat 32 and 64 rows (more CTAs
+// to hide latency with); loading the data only after a warp's vote found void was 4 % slower, and
+// 8 z voxels per thread on 64 x 16 tiles (twice the loads in flight, 6-8 CTAs per SM) 5-15 %.
 constexpr int PD_BY = 16;  // rows per CTA (8 * PD_BY threads)
 __global__ void __launch_bounds__(8 * PD_BY) k_plume_direct(const float* __restrict__ C, float* __restrict__ Cn,
                                                       const uint8_t* __restrict__ M, int nx, int ny, int nz, int mz,
@@ -674,25 +678,23 @@ __global__ void __launch_bounds__(8 * PD_BY) k_plume_direct(const float* __restr
     kw.wt = kw.wb + c.dtp * c.vz_over_dz;
     kw.w0 = 1.0f - 2.0f * (kw.wx + kw.wy + kw.wb) - c.dtp * c.vz_over_dz;
     kw.decay = c.decay;
-    // cw / cc / ce: planes i-1 / i / i+1 of the row, loaded only for planes a warp computes (the
-    // flags are warp-uniform); a plane with nothing to write loads nothing but its mask bytes
-    float4 cw = z4, cc = z4, ce = z4;
-    bool hw = false, hc = false;
+    // planes i-1 / i of the row
+    float4 cw = in && ib > 0 ? __ldg(reinterpret_cast<const float4*>(C + idx - plane)) : z4;
+    float4 cc = in ? __ldg(reinterpret_cast<const float4*>(C + idx)) : z4;
     for (int i = ib; i < ie; ++i, idx += plane, mp += mplane) {
         const unsigned mr = act ? (__ldg(reinterpret_cast<const unsigned*>(mp)) & zkeep) : 0u;
+        const float4 ce = in && i + 1 < nx ? __ldg(reinterpret_cast<const float4*>(C + idx + plane)) : z4;
+        const float4 cs = in && j > 0 ? __ldg(reinterpret_cast<const float4*>(C + idx - nz)) : z4;
+        const float4 cn = in && j + 1 < ny ? __ldg(reinterpret_cast<const float4*>(C + idx + nz)) : z4;
+        float eb = 0.0f, et = 0.0f;
+        if (zg == 0 && in && k > 0) eb = __ldg(C + idx - 1);
+        if (zg == 7 && in && k + 4 < nz) et = __ldg(C + idx + 4);
         const unsigned vd = mr & 0x40404040u;
-        bool he = false;
         if (__any_sync(0xffffffffu, act && (vd || full_write))) {
-            if (!hw) cw = in && i > 0 ? __ldg(reinterpret_cast<const float4*>(C + idx - plane)) : z4;
-            if (!hc) cc = in ? __ldg(reinterpret_cast<const float4*>(C + idx)) : z4;
-            ce = in && i + 1 < nx ? __ldg(reinterpret_cast<const float4*>(C + idx + plane)) : z4;
-            he = true;
-            const float4 cs = in && j > 0 ? __ldg(reinterpret_cast<const float4*>(C + idx - nz)) : z4;
-            const float4 cn = in && j + 1 < ny ? __ldg(reinterpret_cast<const float4*>(C + idx + nz)) : z4;
             float zb = __shfl_up_sync(0xffffffffu, cc.w, 1, 8);
             float zt = __shfl_down_sync(0xffffffffu, cc.x, 1, 8);
-            if (zg == 0) zb = in && k > 0 ? __ldg(C + idx - 1) : 0.0f;
-            if (zg == 7) zt = in && k + 4 < nz ? __ldg(C + idx + 4) : 0.0f;
+            if (zg == 0) zb = eb;
+            if (zg == 7) zt = et;
             float v[4];
             if (__all_sync(0xffffffffu, all_interior(mr) || !act)) {
                 v[0] = ftcs<true>(cc.x, cw.x, ce.x, cs.x, cn.x, zb, cc.y, mr & 0xffu, kw);
@@ -717,9 +719,7 @@ __global__ void __launch_bounds__(8 * PD_BY) k_plume_direct(const float* __restr
             }
         }
         cw = cc;
-        hw = hc;
         cc = ce;
-        hc = he;
     }
 }
 
@@ -1292,7 +1292,8 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     err = nullptr;
 #endif
     // plume kernel: 0 = scalar TMA kernel, 1 / 2 = persistent x-marching kernel, 2 / 4 planes per copy,
-    // 3 = two steps per launch (k_plume_tb, 2 planes per copy; single steps on kernel 1)
+    // 3 = two steps per launch (k_plume_tb, 2 planes per copy; single steps on kernel 1),
+    // 4 = direct (k_plume_direct)
     // (64 registers x 288 threads: at most 3 CTAs per SM; 4 at 56 registers measured slower)
     const int kernel = tune_value(BD_TUNE_PLUME_KERNEL);
     const int shape = kernel >= 3 ? 1 : kernel;  // the one-step kernel (kernel 4 launches its own)
@@ -1311,7 +1312,7 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     int xm_grid = 0, tb_grid = 0;
     int* xm_ext = nullptr;
     unsigned xm_smem = shape == 1 ? PlumeXM<2>::SMEM : PlumeXM<4>::SMEM;
-    if (tma && shape > 0 && kernel != 4) {
+    if (tma && shape > 0 && kernel < 4) {
         int dev = 0, sms = 0, occ = 0;
         BD_CUDA(cudaGetDevice(&dev));
         BD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

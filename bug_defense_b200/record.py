@@ -4,13 +4,16 @@ The production runner pulls full 3-D fields from the engine after every epoch an
 the host (knowledge/beetle/scripts/run_highres_knowledge_suite.py:271-306), then saves one npz per
 run (:330-367). Here bd_engine_record fills a compact record slot on the device (xz slices of T,
 Q, phase and plume absorption, crater depth, band peak temperatures, the epoch's diagnostics), the
-slot is copied asynchronously into a ring of pinned host buffers, and a slot is unpacked only when
-the ring wraps around or at finish(): the GPU never waits for the host.
+slot is copied asynchronously into a ring of pinned host buffers, and filled slots are unpacked
+while the engine waits for its next epoch (the engine's wait hook), when the ring wraps around, or
+at finish(): the GPU never waits for the host, and a synchronising caller (step_epoch after every
+epoch) does not leave the GPU idle while slots are unpacked.
 """
 from __future__ import annotations
 
 import ctypes
 import math
+import weakref
 
 import numpy as np
 import torch
@@ -37,9 +40,13 @@ class Recorder:
         self.slot_bytes = int(_lib.load().bd_record_slot_bytes(self.nx, self.nz))
         self.dev_slot = torch.empty(self.slot_bytes, dtype=torch.uint8, device=eng.dev)
         self.ring = [torch.empty(self.slot_bytes, dtype=torch.uint8, pin_memory=True) for _ in range(int(ring))]
-        self.events = [None] * len(self.ring)
+        self.events = [torch.cuda.Event() for _ in self.ring]
         self.pending = [None] * len(self.ring)       # epoch index held by a ring slot
         self.n = 0
+        self.drained = 0                             # slots are drained in record order
+        hooks = getattr(eng, "_wait_hooks", None)
+        if hooks is not None:
+            hooks.append(weakref.WeakMethod(self._drain_filled))
         self.rows = {}
         gap = getattr(eng, "air_gap_range", None)
         self.gap = (int(gap[0]), int(gap[1])) if gap is not None else (0, 0)
@@ -67,11 +74,18 @@ class Recorder:
                   _lib.stream_ptr(st))
         with torch.cuda.stream(st):
             self.ring[i].copy_(self.dev_slot, non_blocking=True)
-            ev = torch.cuda.Event()
-            ev.record(st)
-        self.events[i] = ev
+        self.events[i].record(st)
         self.pending[i] = self.n
         self.n += 1
+
+    def _drain_filled(self):
+        """Unpack every recorded slot (the engine calls this after enqueuing an epoch, before it
+        blocks: the slots' copies precede that epoch, so the waits end while the epoch runs)."""
+        while self.drained < self.n:
+            i = self.drained % len(self.ring)
+            if self.pending[i] is not None:
+                self._drain(i)
+            self.drained += 1
 
     def _drain(self, i):
         self.events[i].synchronize()
@@ -91,6 +105,7 @@ class Recorder:
         for i in range(len(self.ring)):
             if self.pending[i] is not None:
                 self._drain(i)
+        self.drained = self.n
         return self.arrays()
 
     def arrays(self) -> dict:

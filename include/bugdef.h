@@ -357,7 +357,7 @@ BD_API int bd_engine_record(BdEngine* e, const BdRecordSpec* spec, void* slot, v
                                         limit); photons per thread = n_photons / (grid * 128)          */
 #define BD_TUNE_STENCIL_XC        1  /* x-planes per CTA of the TMA substep kernel, 1..64 (default 8)   */
 #define BD_TUNE_PLUME_XC          2  /* plume kernels 0 and 4: x-planes per CTA; kernels 1-3: CTAs per SM
-                                        (capped by occupancy); 1..64 (default 3)                       */
+                                        (capped by occupancy); 1..64 (default 4)                       */
 #define BD_TUNE_PLUME_KERNEL      3  /* plume step: 0 = one voxel per thread, x chunks per CTA; 1 / 2 =
                                         persistent, four z voxels per thread marching x, 2 / 4 x-planes
                                         per copy; 3 = as 1 with two time steps per launch; 4 = a CTA per

@@ -63,10 +63,11 @@ def test_launch_shapes_leave_results_bit_identical(gpu, restore_knobs):
 
 
 def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
-    """The scalar plume kernel (several x-chunk lengths) and the persistent x-marching kernel
-    (several grid sizes, i.e. run splits) give the same bits: through the context API (full writes
-    on the first steps, ragged y tiles, scattered void) and through the engine (void z-limit,
-    partly void 4-voxel groups at the crater walls, bulk-void fast path)."""
+    """Every plume kernel gives the same bits: the scalar kernel (several x-chunk lengths), the
+    persistent x-marching kernels (several grid sizes, i.e. run splits) and the direct kernel
+    (several x-chunk lengths), through the context API (full writes on the first steps, ragged y
+    tiles, scattered void, a partly filled last z tile) and through the engine (void z-limit,
+    partly void voxel groups at the crater walls, bulk-void fast path)."""
     from bug_defense_b200 import _lib, campaign
     rng = np.random.default_rng(11)
     scattered = rng.uniform(size=(9, 35, 68)) < 0.7
@@ -76,12 +77,16 @@ def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
     cavity = np.zeros((12, 70, 132), bool)              # deep z tiles void only in a small cavity, the
     cavity[:, :, :40] = True                            # deepest none: trimmed and empty columns
     cavity[3:7, 20:41, 70:101] = True
-    for vd in (scattered, slab, cavity):
+    cavity8 = np.zeros((11, 37, 136), bool)             # last 32-voxel z tile 8 deep, ragged y tiles
+    cavity8[:, :, :44] = True
+    cavity8[2:9, 5:30, 60:131] = rng.uniform(size=(7, 25, 71)) < 0.8
+    for vd in (scattered, slab, cavity, cavity8):
         shape = vd.shape
         C0 = (rng.uniform(0, 1, shape) * vd).astype(np.float32)
         z = np.zeros(shape)
         fields = []
-        for kern, xc in ((0, 4), (0, 2), (1, 4), (1, 1), (2, 2), (2, 1), (1, 3), (3, 2), (3, 1), (4, 2)):
+        for kern, xc in ((0, 4), (0, 2), (1, 4), (1, 1), (2, 2), (2, 1), (1, 3), (3, 2), (3, 1), (4, 2),
+                         (4, 1), (4, 3)):
             _knob(_lib.TUNE_PLUME_KERNEL, kern)
             _knob(_lib.TUNE_PLUME_XC, xc)
             ctx = gpu.MetalAblationContext(*shape, 0.03, 0.025, 0.02, 1e-5, 0.0, 20.0, 100.0, 300.0,
