@@ -146,10 +146,19 @@ __global__ void __launch_bounds__(256) k_void_plume(PhaseArgs a, long long nv) {
     float peak = 0.0f;
     int kmax = -1;
     unsigned long long n_void = 0;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv;
-         i += (long long)gridDim.x * blockDim.x) {
+    // (column, z) of voxel i, stepped with the grid stride instead of two 64-bit divisions per voxel
+    const long long i0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const int sk = (int)(stride % a.nz);
+    const long long sc = stride / a.nz;
+    long long col = i0 / a.nz;
+    int k = (int)(i0 - col * a.nz);
+    for (long long i = i0; i < nv; i += stride, col += sc, k += sk) {
+        if (k >= a.nz) {
+            k -= a.nz;
+            ++col;
+        }
         uint8_t f = a.flags[i];
-        const int k = (int)(i % a.nz);
         const bool ablated = (f & BD_FLAG_ABLATED) != 0;
         const bool vd = ablated || (gap_open && k >= a.gap_k0 && k < a.gap_k1);
         f = vd ? (uint8_t)(f | BD_FLAG_VOID) : (uint8_t)(f & ~BD_FLAG_VOID);
@@ -168,7 +177,7 @@ __global__ void __launch_bounds__(256) k_void_plume(PhaseArgs a, long long nv) {
             a.mu_ext[i] = mu_ext;
             const float mua_p = mu_ext * a.ratio_a;
             peak = fmaxf(peak, mua_p);
-            if ((long long)(i / a.nz) == mid_col) tau_sum += (double)mua_p;
+            if (col == mid_col) tau_sum += (double)mua_p;
             if (ablated) { abl_sum += (double)mua_p; abl_cnt += 1.0; }
         } else if (ablated) {
             abl_cnt += 1.0;
