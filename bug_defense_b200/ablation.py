@@ -7,7 +7,7 @@ plume transport in the void domain (bd_plume_advance). The plume does not feed b
 thermal fields inside a substep (metal_ablation_solver.py:193-240 only reads plume buffers), so
 it runs as its own kernel sequence over the same substeps.
 
-Semantic switches (defaults reproduce the reference CPU solvers, which judge parity):
+Semantic switches (defaults reproduce the reference CPU solvers, the parity reference):
   bc:               'series' (voxel_thermal_3d.py:97,105) or 'metal' (metal_ablation_solver.py:141,150)
   plume_dt_policy:  'as_given' (plume.py:79), 'metal' (dt clamp, metal_ablation_solver.py:235-237)
                     or 'subcycle' (stable sub-steps of dt/n_sub)

@@ -6,7 +6,7 @@ CoupledAblationEngine.step_epoch pays for the photon count that makes them smoot
 (coupled_ablation.py:454-468). This module adds a small 3-D U-Net (3 levels, 16/32/64 channels,
 BF16 tensor-core convolutions with FP32 accumulation) that maps a map traced with few photons,
 plus the optical properties and tissue state, to an estimate of the many-photon map. Plain MC stays
-the fallback and the judge of its error.
+the fallback and the reference for its error.
 
 Volumes on the device are bf16 "8-channel planes" with a one-voxel zero pad (see
 include/bugdef.h, "Absorbed-map denoiser"). This module holds the layer-level wrappers of the C ABI

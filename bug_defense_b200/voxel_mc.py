@@ -279,7 +279,7 @@ def run_voxel_mc3d(power: float = 1.0, pulse_duration: float = 0.20, n_photons: 
                    launch_axis: str = 'z', beam_center=None, beam_profile: str = 'gaussian',
                    engine: str = 'auto', base_seed: int = None, semantics: str = 'cpu', device=None) -> dict:
     """Signature of simulation/voxel_mc_3d.py:425-445. engine 'auto' and 'gpu' run the CUDA
-    kernel; this build ships no CPU engine, so engine='cpu' raises ValueError."""
+    kernel; this package ships no CPU engine, so engine='cpu' raises ValueError."""
     eng = str(engine).strip().lower()
     if eng not in ('auto', 'gpu', 'cpu'):
         raise ValueError(f"Unknown engine='{engine}'. Valid options: 'auto', 'gpu', 'cpu'.")

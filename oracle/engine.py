@@ -1,7 +1,7 @@
 """ORACLE -- test infrastructure only: FP64 CPU restatement of CoupledAblationEngine.step_epoch
 (simulation/coupled_ablation.py:440-617, CPU thermal path :507-544) on the C kernels of
 oracle/orc.c, with the reference's host logic (removal :628-660, void mask :619-626, plume
-inject/sync plume.py:292-366) in numpy. Used as the checker and as the timed CPU port
+inject/sync plume.py:292-366) in numpy. Used as the parity reference and as the timed CPU port
 (bench.py --impl reference / cpu_baseline); never imported by the product."""
 from __future__ import annotations
 

@@ -1,7 +1,7 @@
 /*
  * ORACLE -- test infrastructure only. A plain-C, FP64 restatement of the reference CPU
  * (numba) kernels of yudovsky/bug-defense, used by tests/, __graft_entry__.smoke() and the
- * cpu_baseline / --impl reference legs of bench.py as the checker and the timed CPU port.
+ * cpu_baseline / --impl reference legs of bench.py as the parity reference and the timed CPU port.
  * Nothing in the product (bug_defense_b200/) links, imports or calls this file.
  *
  * Pinning: tests/golden/ holds fixtures produced by running the reference itself
