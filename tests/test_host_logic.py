@@ -94,3 +94,31 @@ def test_gpu_only_build_rejects_cpu_engine_and_missing_device():
         # the product has no CPU fallback: without a device it raises
         with pytest.raises(RuntimeError):
             voxel_mc.run_voxel_mc3d(n_photons=10, engine='gpu', Nx=4, Ny=4, Nz=4)
+
+
+def test_engine_wait_hooks_run_once_each_and_drop_dead_owners():
+    """Host work registered with an engine (the Recorder's slot unpacking) runs each time the engine
+    is about to block on an epoch's diagnostics; a hook whose owner was collected is dropped."""
+    import gc
+    import weakref
+    from bug_defense_b200.coupled import CoupledAblationEngine
+
+    calls = []
+
+    class Owner:
+        def __init__(self, tag):
+            self.tag = tag
+
+        def hook(self):
+            calls.append(self.tag)
+
+    eng = object.__new__(CoupledAblationEngine)      # host logic only: no device state
+    eng._wait_hooks = []
+    a, b = Owner("a"), Owner("b")
+    eng._wait_hooks += [weakref.WeakMethod(a.hook), weakref.WeakMethod(b.hook)]
+    eng._run_wait_hooks()
+    assert calls == ["a", "b"]
+    del b
+    gc.collect()
+    eng._run_wait_hooks()
+    assert calls == ["a", "b", "a"] and len(eng._wait_hooks) == 1
