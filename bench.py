@@ -285,7 +285,7 @@ def ours_main(args):
     kv = ctypes.c_int(0)
     _lib.call("bd_tune_get", _lib.TUNE_PLUME_KERNEL, ctypes.byref(kv))
     plume_kernel = {0: "k_plume_step_tma", 1: "k_plume_xm<2>", 2: "k_plume_xm<4>",
-                    3: "k_plume_tb<2>", 4: "k_plume_direct"}.get(kv.value, "k_plume_step")
+                    3: "k_plume_tb<2>", 4: "k_plume_direct_z"}.get(kv.value, "k_plume_step")
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
@@ -314,9 +314,9 @@ def ours_main(args):
             mc["photon_steps_per_s"] = steps_per_epoch * r["n_on"] / (mc_ms * 1e-3)
         lc = (ld[1:7].sum() + ld[8] + ld[9] - ld[7]) / max(ld[0], 1)
         mc["ledger_closure_minus_1"] = float(lc - 1.0)
-    # per epoch: begin + 3 epoch-end kernels + substeps + plume steps; per laser epoch: MC, ledger
-    # reduction and tally finalisation
-    gpu_launches = K * (1 + 3 + eng.n_substeps + eng.n_substeps * n_plume_sub) + r["n_on"] * 3
+    # per epoch: begin + 3 epoch-end kernels + plume mask + plume z lists + substeps + plume steps;
+    # per laser epoch: MC, ledger reduction and tally finalisation
+    gpu_launches = K * (1 + 3 + 2 + eng.n_substeps + eng.n_substeps * n_plume_sub) + r["n_on"] * 3
     out = {"metric": METRIC, "value": round(value, 3), "unit": "epochs/s", "n_gpus": world, "steps": K,
            "warmup": args.warmup, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32 (FP64 ledgers)", "data": "synthetic (seeded, reference config shapes)",

@@ -30,8 +30,19 @@ constexpr int kPlumeMaxCols = 1024;
 inline size_t plume_mask_only_bytes(int nx, int ny, int nz) {
     return ((size_t)nx * ny * plume_mask_pitch(nz) + 255) / 256 * 256;
 }
-inline size_t plume_mask_bytes(int nx, int ny, int nz) {
+// Then the live z groups of the direct plume kernel's columns (x chunk, 16-row y tile): one count
+// byte per column, then per column the ascending ids of its 4-voxel z groups that hold void
+// (at most (nz + 3) / 4 <= 255 ids; sized for one x plane per chunk).
+constexpr int kPlumeZRows = 16;
+inline size_t plume_zlist_offset(int nx, int ny, int nz) {
     return plume_mask_only_bytes(nx, ny, nz) + sizeof(int) * (3 * kPlumeMaxCols + 1);
+}
+inline size_t plume_zlist_bytes(int nx, int ny, int nz) {
+    const size_t cols = (size_t)nx * ((ny + kPlumeZRows - 1) / kPlumeZRows);
+    return (cols * (1 + (size_t)(nz + 3) / 4) + 255) / 256 * 256;
+}
+inline size_t plume_mask_bytes(int nx, int ny, int nz) {
+    return plume_zlist_offset(nx, ny, nz) + plume_zlist_bytes(nx, ny, nz);
 }
 
 // Launch-shape knobs (BD_TUNE_*) and the generation counter bumped by every change.

@@ -723,6 +723,134 @@ __global__ void __launch_bounds__(8 * PD_BY) k_plume_direct(const float* __restr
     }
 }
 
+static_assert(PD_BY == kPlumeZRows, "z-list columns follow the direct kernel's y tiles");
+
+// Live z groups of every (x chunk, y tile) column of the direct kernel: a CTA per column (grid
+// n_yt x n_chunks), thread g = the 4-voxel z group g; live when any of the column's planes and rows
+// holds a void voxel in the group below the void z-limit (the mask bytes at or above it are not
+// rebuilt, so they are masked off here). The void domain is fixed within a plume stage, so the
+// lists are built once per stage, after the mask.
+__global__ void __launch_bounds__(256) k_plume_zlist(const uint8_t* __restrict__ M, int nx, int ny, int nz, int mz,
+                                                     int xc, const int* __restrict__ zlimit,
+                                                     uint8_t* __restrict__ zlist) {
+    __shared__ int wcount[8];
+    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
+    const int G = (nz + 3) / 4;
+    const int n_yt = gridDim.x;
+    const int n_cols = gridDim.x * gridDim.y;
+    const int col = blockIdx.y * n_yt + blockIdx.x;
+    const int ib = blockIdx.y * xc, ie = min(nx, ib + xc);
+    const int j0 = blockIdx.x * PD_BY, j1 = min(ny, j0 + PD_BY);
+    const int g = threadIdx.x;
+    const int nk = zl - 4 * g;
+    bool live = false;
+    if (g < G && nk > 0) {
+        const unsigned keep = nk >= 4 ? 0xffffffffu : (0xffffffffu >> (8 * (4 - nk)));
+        for (int i = ib; i < ie && !live; ++i)
+            for (int j = j0; j < j1; ++j)
+                if (__ldg(reinterpret_cast<const unsigned*>(M + ((size_t)i * ny + j) * mz + 4 * g)) & keep &
+                    0x40404040u) {
+                    live = true;
+                    break;
+                }
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, live);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) wcount[w] = __popc(bal);
+    __syncthreads();
+    int before = 0;
+    for (int q = 0; q < w; ++q) before += wcount[q];
+    if (live) zlist[n_cols + (size_t)col * G + before + __popc(bal & ((1u << lane) - 1u))] = (uint8_t)g;
+    if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int q = 0; q < 8; ++q) tot += wcount[q];
+        zlist[col] = (uint8_t)tot;
+    }
+}
+
+// Direct plume step over the live z groups only (steps after the first two of a stage): as
+// k_plume_direct, but band blockIdx.x of a column takes the column's live groups 8 b .. 8 b + 7
+// from its z list instead of 8 consecutive groups, so z tiles that are partly tissue cost only
+// their void groups. A lane whose z neighbour group is not held by the neighbouring lane loads
+// that neighbour voxel instead of taking it by shuffle. Same per-voxel expression (bit-identical);
+// voxels outside the lists are not void and are written by no step after the first two.
+__global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_z(const float* __restrict__ C, float* __restrict__ Cn,
+                                                        const uint8_t* __restrict__ M, int nx, int ny, int nz,
+                                                        int mz, int xc, PlumeConst c, const int* __restrict__ zlimit,
+                                                        const uint8_t* __restrict__ zlist) {
+    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
+    const int G = (nz + 3) / 4;
+    const int n_cols = gridDim.y * gridDim.z;
+    const int col = blockIdx.z * gridDim.y + blockIdx.y;
+    const int cnt = zlist[col];
+    const int b0 = blockIdx.x * 8;
+    const int ib = blockIdx.z * xc, ie = min(nx, ib + xc);
+    if (b0 >= cnt || ib >= ie) return;  // uniform over the CTA
+    const int zg = threadIdx.x & 7;
+    const int g = b0 + zg < cnt ? (int)zlist[n_cols + (size_t)col * G + b0 + zg] : -2;
+    const int gp = __shfl_up_sync(0xffffffffu, g, 1, 8);
+    const int gn = __shfl_down_sync(0xffffffffu, g, 1, 8);
+    const bool zb_lane = zg > 0 && gp == g - 1;  // the -z neighbour is the previous lane's last voxel
+    const bool zt_lane = zg < 7 && gn == g + 1;  // the +z neighbour is the next lane's first voxel
+    const int j = blockIdx.y * PD_BY + (threadIdx.x >> 3), k = 4 * max(g, 0);
+    const int nk = zl - k;
+    const bool act = g >= 0 && nk > 0 && j < ny;
+    const bool in = g >= 0 && j < ny && k < nz;
+    const unsigned zkeep = nk >= 4 ? 0xffffffffu : (nk <= 0 ? 0u : (0xffffffffu >> (8 * (4 - nk))));
+    const size_t plane = (size_t)ny * nz;
+    const size_t mplane = (size_t)ny * mz;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    size_t idx = ((size_t)ib * ny + j) * nz + k;
+    const uint8_t* mp = M + ((size_t)ib * ny + j) * mz + k;
+    PlumeW kw;
+    kw.wx = c.dtp * c.dxy_x; kw.wy = c.dtp * c.dxy_y; kw.wb = c.dtp * c.dz_z;
+    kw.wt = kw.wb + c.dtp * c.vz_over_dz;
+    kw.w0 = 1.0f - 2.0f * (kw.wx + kw.wy + kw.wb) - c.dtp * c.vz_over_dz;
+    kw.decay = c.decay;
+    float4 cw = in && ib > 0 ? __ldg(reinterpret_cast<const float4*>(C + idx - plane)) : z4;
+    float4 cc = in ? __ldg(reinterpret_cast<const float4*>(C + idx)) : z4;
+    for (int i = ib; i < ie; ++i, idx += plane, mp += mplane) {
+        const unsigned mr = act ? (__ldg(reinterpret_cast<const unsigned*>(mp)) & zkeep) : 0u;
+        const float4 ce = in && i + 1 < nx ? __ldg(reinterpret_cast<const float4*>(C + idx + plane)) : z4;
+        const float4 cs = in && j > 0 ? __ldg(reinterpret_cast<const float4*>(C + idx - nz)) : z4;
+        const float4 cn = in && j + 1 < ny ? __ldg(reinterpret_cast<const float4*>(C + idx + nz)) : z4;
+        float eb = 0.0f, et = 0.0f;
+        if (!zb_lane && in && k > 0) eb = __ldg(C + idx - 1);
+        if (!zt_lane && in && k + 4 < nz) et = __ldg(C + idx + 4);
+        const unsigned vd = mr & 0x40404040u;
+        if (__any_sync(0xffffffffu, act && vd)) {
+            float zb = __shfl_up_sync(0xffffffffu, cc.w, 1, 8);
+            float zt = __shfl_down_sync(0xffffffffu, cc.x, 1, 8);
+            if (!zb_lane) zb = eb;
+            if (!zt_lane) zt = et;
+            float v[4];
+            if (__all_sync(0xffffffffu, all_interior(mr) || !act)) {
+                v[0] = ftcs<true>(cc.x, cw.x, ce.x, cs.x, cn.x, zb, cc.y, mr & 0xffu, kw);
+                v[1] = ftcs<true>(cc.y, cw.y, ce.y, cs.y, cn.y, cc.x, cc.z, (mr >> 8) & 0xffu, kw);
+                v[2] = ftcs<true>(cc.z, cw.z, ce.z, cs.z, cn.z, cc.y, cc.w, (mr >> 16) & 0xffu, kw);
+                v[3] = ftcs<true>(cc.w, cw.w, ce.w, cs.w, cn.w, cc.z, zt, mr >> 24, kw);
+            } else {
+                v[0] = ftcs<false>(cc.x, cw.x, ce.x, cs.x, cn.x, zb, cc.y, mr & 0xffu, kw);
+                v[1] = ftcs<false>(cc.y, cw.y, ce.y, cs.y, cn.y, cc.x, cc.z, (mr >> 8) & 0xffu, kw);
+                v[2] = ftcs<false>(cc.z, cw.z, ce.z, cs.z, cn.z, cc.y, cc.w, (mr >> 16) & 0xffu, kw);
+                v[3] = ftcs<false>(cc.w, cw.w, ce.w, cs.w, cn.w, cc.z, zt, mr >> 24, kw);
+            }
+            if (act && vd) {
+                float* dst = Cn + idx;
+                if (vd == 0x40404040u) {
+                    *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                        if (vd & (0x40u << (8 * e))) dst[e] = v[e];
+                }
+            }
+        }
+        cw = cc;
+        cc = ce;
+    }
+}
+
 template <int PB>
 __global__ void __launch_bounds__(PX_THREADS, 1) k_plume_xm(const __grid_constant__ CUtensorMap c_map,
                                                          const __grid_constant__ CUtensorMap m_map,
@@ -1293,7 +1421,8 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
 #endif
     // plume kernel: 0 = scalar TMA kernel, 1 / 2 = persistent x-marching kernel, 2 / 4 planes per copy,
     // 3 = two steps per launch (k_plume_tb, 2 planes per copy; single steps on kernel 1),
-    // 4 = direct (k_plume_direct)
+    // 4 = direct: k_plume_direct_z over each column's live z groups, k_plume_direct for the first
+    //     two (full-write) steps and for nz > 1020
     // (64 registers x 288 threads: at most 3 CTAs per SM; 4 at 56 registers measured slower)
     const int kernel = tune_value(BD_TUNE_PLUME_KERNEL);
     const int shape = kernel >= 3 ? 1 : kernel;  // the one-step kernel (kernel 4 launches its own)
@@ -1347,6 +1476,14 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
             tb_grid = (int)std::max(1LL, std::min(planes2, (long long)std::max(std::min(occ2, xc), 1) * sms));
         }
     }
+    // live z groups per direct-kernel column, from this stage's mask (steps after the first two)
+    uint8_t* zlist = nullptr;
+    if (tma && kernel == 4 && (p->nz + 3) / 4 <= 255) {
+        zlist = mask + plume_zlist_offset(p->nx, p->ny, p->nz);
+        k_plume_zlist<<<dim3((p->ny + PD_BY - 1) / PD_BY, (p->nx + xc - 1) / xc), 256, 0, st>>>(
+            mask, p->nx, p->ny, p->nz, mz, xc, full_first ? nullptr : zlimit, zlist);
+        BD_CHECK_LAUNCH("k_plume_zlist");
+    }
     const long long total = (long long)steps * n_substeps;
     long long launches = 0;  // each launch moves the field to the other buffer
     for (long long s = 0; s < total;) {
@@ -1357,6 +1494,12 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
         const CUtensorMap& map = odd ? map_b : map_a;
         const int* zl = full ? nullptr : zlimit;
         ++launches;
+        if (kernel == 4 && tma && zlist && !full) {
+            ++s;
+            k_plume_direct_z<<<dim3((p->nz + PL_BZ - 1) / PL_BZ, (p->ny + PD_BY - 1) / PD_BY, (p->nx + xc - 1) / xc),
+                               8 * PD_BY, 0, st>>>(in, out, mask, p->nx, p->ny, p->nz, mz, xc, c, zl, zlist);
+            continue;
+        }
         if (kernel == 4 && tma) {
             ++s;
             k_plume_direct<<<dim3((p->nz + PL_BZ - 1) / PL_BZ, (p->ny + PD_BY - 1) / PD_BY, (p->nx + xc - 1) / xc),

@@ -361,7 +361,9 @@ BD_API int bd_engine_record(BdEngine* e, const BdRecordSpec* spec, void* slot, v
 #define BD_TUNE_PLUME_KERNEL      3  /* plume step: 0 = one voxel per thread, x chunks per CTA; 1 / 2 =
                                         persistent, four z voxels per thread marching x, 2 / 4 x-planes
                                         per copy; 3 = as 1 with two time steps per launch; 4 = a CTA per
-                                        32 x 16 tile marching x planes, no staging (default 4)         */
+                                        32 x 16 tile marching x planes, no staging, over each tile
+                                        column's live z groups after a stage's first two steps
+                                        (default 4)                                                     */
 #define BD_TUNE_COUNT             4
 BD_API int bd_tune_set(int knob, int value);
 BD_API int bd_tune_get(int knob, int* value);

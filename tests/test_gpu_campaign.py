@@ -86,7 +86,7 @@ def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
         z = np.zeros(shape)
         fields = []
         for kern, xc in ((0, 4), (0, 2), (1, 4), (1, 1), (2, 2), (2, 1), (1, 3), (3, 2), (3, 1), (4, 2),
-                         (4, 1), (4, 3)):
+                         (4, 1), (4, 3), (4, 4)):
             _knob(_lib.TUNE_PLUME_KERNEL, kern)
             _knob(_lib.TUNE_PLUME_XC, xc)
             ctx = gpu.MetalAblationContext(*shape, 0.03, 0.025, 0.02, 1e-5, 0.0, 20.0, 100.0, 300.0,
