@@ -52,10 +52,8 @@ def parse():
 
 
 def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", str(rank)))
-    return rank, world, local
+    from bug_defense_b200.replicas import dist_env as env
+    return env()
 
 
 def measured_peaks():
@@ -172,7 +170,8 @@ def run_ours(args, rank, world, local):
             return e
         tuned = campaign.autotune(probe)
         torch.cuda.synchronize()
-    eng = make_engine(geo, dev, seed_offset=rank)
+    from bug_defense_b200.replicas import replica_seed
+    eng = make_engine(geo, dev, seed_offset=replica_seed(0, rank))
     K, W = int(args.steps), int(args.warmup)
     n_on = max(1, int(round(LASER_DUTY * K)))
     for _ in range(W):
@@ -203,10 +202,8 @@ def run_ours(args, rank, world, local):
     lib.bd_engine_timing(eng._handle, 0)
     stage_ms = list(stage)
     d = eng._diag(None)
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    from bug_defense_b200.replicas import max_over_ranks
+    ms = max_over_ranks(ms, device=dev)
     res = {"ms": ms, "K": K, "n_on": n_on, "stage_ms": stage_ms, "clocks": clk.summary(), "eng": eng, "geo": geo,
            "last_diag": d, "laser_diag": laser_diag, "tuned": tuned}
     return res
@@ -365,10 +362,19 @@ def campaign_main(args):
     """24 instances (8 wavelengths x 3 powers, pulse U(50, 400) ms) of the full-resolution run at
     once; a step is one 1 ms epoch of every instance. Launch shapes from the autotuner."""
     import torch
+    import torch.distributed as dist
     from bug_defense_b200 import campaign
+    from bug_defense_b200.replicas import max_over_ranks, rank_share, sum_over_ranks
     rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    insts = [i for i in campaign.campaign_instances(args.seed) if i["index"] % world == rank]
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    all_insts = campaign.campaign_instances(args.seed)
+    if world > len(all_insts):
+        raise ValueError(f"{world} ranks for {len(all_insts)} campaign instances")
+    insts = rank_share(all_insts, rank, world)
     t0 = time.perf_counter()
     tuned = campaign.autotune(insts[0])
     t_tune = time.perf_counter() - t0
@@ -377,6 +383,8 @@ def campaign_main(args):
     camp.diagnostics()
     K = int(args.steps)
     torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     # every instance stream waits for ev0 and ev1 waits for every stream: device-timed makespan
     ev0.record()
@@ -391,15 +399,17 @@ def campaign_main(args):
         torch.cuda.current_stream().wait_stream(st)
     ev1.record()
     torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
+    # whole job: every rank's instances over the slowest rank's device-timed makespan
+    ms = max_over_ranks(ev0.elapsed_time(ev1), device=dev)
+    n_inst = int(sum_over_ranks(len(insts), device=dev))
     diags = camp.diagnostics()
-    value = len(insts) * K / (ms / 1e3)
+    value = n_inst * K / (ms / 1e3)
     out = {"metric": "campaign instance-epochs/s (24 full-resolution instances at once)", "value": round(value, 3),
            "unit": "instance-epochs/s", "n_gpus": world, "steps": K, "warmup": args.warmup,
            "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
            "dtype": "f32 (FP64 ledgers)", "data": "synthetic (seeded, reference config shapes)",
            "config": {"workload": "campaign: 8 wavelengths x 3 powers, pulse U(50, 400) ms, 200x200x192 @ 15 um, "
-                                  "150k photons per laser epoch", "instances": len(insts),
+                                  "150k photons per laser epoch", "instances": n_inst,
                       "parallelism": f"instances split over {world} rank(s)"},
            "autotune": {k: v for k, v in tuned.items()}, "autotune_s": round(t_tune, 1),
            "setup_s": round(camp.setup_s, 1),
@@ -407,6 +417,9 @@ def campaign_main(args):
            "impl": "ours"}
     if rank == 0:
         print(json.dumps(out))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def reference_main(args):
