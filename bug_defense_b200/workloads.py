@@ -7,6 +7,7 @@ to voxels by the cell-centre rule (simulation/voxel_mc_3d.py:527-536).
   single_epoch_stack(seed)  64x64x128 at 15 um: one 20k-photon epoch + 20 substeps, no ablation
   full_coupled_run(seed)    200x200x128 stack + 64 air slices on top (the plume region) = 200x200x192;
                             boiling, char, ablation, plume; 150k photons per epoch
+  crater_sample(seed)       a random crater on the 200x200x128 stack (denoiser training / evaluation)
 """
 from __future__ import annotations
 
@@ -149,6 +150,17 @@ def engine_kwargs(geo: dict) -> dict:
                 plume_closure=geo["plume_closure"], initial_dry_mask=geo["dry_mask"],
                 initial_ablated_mask=geo["ablated_mask"], air_gap_range=geo["air_gap_range"],
                 wavelength_nm=532.0, seed=geo["seed"] + 1)
+
+
+def single_epoch_kwargs(geo: dict, seed: int = 1) -> dict:
+    """CoupledAblationEngine keyword arguments of the single-epoch stack (single_epoch_stack): the
+    same optics, conduction and beam, with boiling and removal out of reach (t_abl 1e9 C, h_lat
+    1e12 J/mm^3, no dry / char state) and no plume, so an epoch is one MC pass + 20 substeps."""
+    return dict(optical_props=geo["optical"], k_grid=geo["k_grid"], rho_cp_grid=geo["rho_cp_grid"],
+                h_lat_grid=geo["h_lat_grid"], Lx=geo["Lx"], Ly=geo["Ly"], Lz=geo["Lz"], power=geo["power"],
+                spot_dia=geo["spot_dia"], t_abl=1e9, t_ambient=25.0, dt_epoch=geo["n_substeps"] * geo["dt_sub"],
+                dt_sub=geo["dt_sub"], n_photons=geo["n_photons"], h_eff=15e-6, theta_inc_deg=geo["theta_inc_deg"],
+                initial_ablated_mask=geo["ablated_mask"], wavelength_nm=532.0, seed=seed)
 
 
 def crater_sample(seed: int, nx: int = 200, ny: int = 200, nz: int = 128, device=None) -> dict:

@@ -209,8 +209,9 @@ BEAM = {'gaussian': 0, 'tophat': 1, 'kim_exp_disk': 2, 'kim_gauss_disk': 3}
 def run_voxel_mc3d(power=1.0, pulse_duration=0.20, n_photons=200000, spot_dia=0.50, theta_inc_deg=0.0,
                    phi_inc_deg=0.0, Lx=4.0, Ly=4.0, Lz=2.42, Nx=80, Ny=80, Nz=60, r_max=0.0, layers_config=None,
                    custom_3d_props=None, launch_axis='z', beam_center=None, beam_profile='gaussian', seed=1,
-                   semantics='cpu', n_chunks=None, tally_fluence=True, max_events=10_000_000):
-    """FP64 restatement of run_voxel_mc3d (voxel_mc_3d.py:425-717) with a seedable Philox RNG."""
+                   semantics='cpu', n_chunks=None, tally_fluence=True, max_events=10_000_000, photon_offset=0):
+    """FP64 restatement of run_voxel_mc3d (voxel_mc_3d.py:425-717) with a seedable Philox RNG.
+    Photon p draws from the Philox stream (seed, photon_offset + p), as the GPU tracer does."""
     dx, dy, dz = Lx / Nx, Ly / Ny, Lz / Nz
     axis = launch_axis.strip().lower()
     if custom_3d_props is not None:
@@ -254,7 +255,7 @@ def run_voxel_mc3d(power=1.0, pulse_duration=0.20, n_photons=200000, spot_dia=0.
     P.sigma, P.radius = w0 / 2.0, w0
     P.n_amb = 1.0
     P.rmax2 = r_max * r_max if r_max > 0 else 0.0
-    P.n_photons, P.offset, P.max_events, P.seed = int(n_photons), 0, int(max_events), int(seed)
+    P.n_photons, P.offset, P.max_events, P.seed = int(n_photons), int(photon_offset), int(max_events), int(seed)
     nv = Nx * Ny * Nz
     if n_chunks is None:
         budget = 512 * 1024 ** 2  # MC3D_SCORING_MEMORY_BUDGET_BYTES (voxel_mc_3d.py:28, :621-625)

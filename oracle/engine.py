@@ -27,7 +27,8 @@ class OracleEngine:
                  beam_center=None, stability_factor=0.35, k_void=K_AIR, rho_cp_void=RHO_CP_AIR, arrhenius=None,
                  beam_profile='gaussian', dry_state=None, char_state=None, plume_closure=None, theta_inc_deg=0.0,
                  phi_inc_deg=0.0, initial_dry_mask=None, initial_ablated_mask=None, air_gap_range=None,
-                 wavelength_nm=10600.0, seed=1, plume_dt_policy='as_given', **_ignored):
+                 wavelength_nm=10600.0, seed=1, plume_dt_policy='as_given', mc_stream='oracle', bc='series',
+                 semantics='cpu', **_ignored):
         self.optical = {k: np.array(optical_props[k], dtype=np.float64, copy=True) for k in ('mu_a', 'mu_s', 'g', 'n')}
         self.Nx, self.Ny, self.Nz = self.optical['mu_a'].shape
         self.Lx, self.Ly, self.Lz = float(Lx), float(Ly), float(Lz)
@@ -100,6 +101,14 @@ class OracleEngine:
                 v=float(pc.get('v_drift', pc.get('vz', 80.0))), tau=float(pc.get('tau_linger_s', 0.00875)),
                 raw=np.zeros(shape), mu_ext=np.zeros(shape))
         self.plume_dt_policy = plume_dt_policy
+        # 'engine': epoch e traces photon p on the Philox stream (seed, (e << 32) + p), the streams of
+        # the GPU engine's epoch e (k_epoch_begin), so the two MC tallies are correlated samples
+        self.mc_stream = mc_stream
+        # z-wall flux of the fused substep (0: series half-cell + h_eff, 1: Metal -h_eff (T - T_amb)) and
+        # the MC semantics (the CPU or the Metal tracer's thresholds)
+        self.bc_mode = {'series': 0, 'cpu': 0, 'metal': 1}[bc]
+        self.semantics = semantics
+        self.last_mc = None
         self._init_ds_cs()
         self.t = 0.0
         self.epoch = 0
@@ -140,7 +149,30 @@ class OracleEngine:
         ra = p['mu_a_max'] / max(1e-6, p['mu_max']); rs = p['mu_s_max'] / max(1e-6, p['mu_max'])
         return p['mu_ext'] * ra, p['mu_ext'] * rs
 
-    def step_epoch(self, absorbed_map=None, threads=None) -> dict:
+    def load_state(self, st: dict):
+        """Overwrite the evolving state with `st` (float64 / bool arrays, e.g. another engine's
+        state after an epoch), so one epoch of both engines can be compared from the same start.
+        Keys: T H_acc chi dry ablated mu_a mu_s g n k_grid rho_cp_grid wet_mu_a wet_k wet_rho_cp T_peak
+        ablation_time t epoch, optionally Omega, and plume_raw plume_mu_ext when there is a plume."""
+        c = lambda a, dt=np.float64: np.array(a, dtype=dt, copy=True).reshape(self.T.shape)
+        self.T, self.H_acc, self.chi = c(st['T']), c(st['H_acc']), c(st['chi'])
+        if 'Omega' in st:
+            self.Omega = c(st['Omega'])
+        self.dry, self.ablated = c(st['dry'], np.bool_), c(st['ablated'], np.bool_)
+        for key in ('mu_a', 'mu_s', 'g', 'n'):
+            self.optical[key] = c(st[key])
+        self.k_grid, self.rho_cp_grid = c(st['k_grid']), c(st['rho_cp_grid'])
+        if self._wet is not None:
+            self._wet = (c(st['wet_mu_a']), c(st['wet_k']), c(st['wet_rho_cp']))
+        self.T_peak, self.ablation_time = c(st['T_peak']), c(st['ablation_time'])
+        self.t, self.epoch = float(st['t']), int(st['epoch'])
+        if self.plume is not None:
+            self.plume['raw'], self.plume['mu_ext'] = c(st['plume_raw']), c(st['plume_mu_ext'])
+        self._T_next = np.empty_like(self.T)
+
+    def step_epoch(self, absorbed_map=None, threads=None, capture=None) -> dict:
+        """One epoch. `capture` (a dict) receives copies of T, H_acc, chi, dry and ablated after the
+        substeps and before the epoch-end phase update (the state the removal rule reads)."""
         t0 = time.perf_counter()
         if self.power > 0.0:
             if absorbed_map is None:
@@ -151,11 +183,16 @@ class OracleEngine:
                     opt['mu_a'] = self.optical['mu_a'] + ma
                     opt['mu_s'] = self.optical['mu_s'] + ms
                     opt['g'][(self.plume['mu_ext'] > 0.001) & self.ablated] = 0.80
+                if self.mc_stream == 'engine':
+                    stream = dict(seed=self.seed, photon_offset=(self.epoch + 1) << 32)
+                else:
+                    stream = dict(seed=self.seed * 1_000_003 + self.epoch)
                 mc = run_voxel_mc3d(power=self.power, n_photons=self.n_photons, spot_dia=self.spot_dia, Lx=self.Lx,
                                     Ly=self.Ly, Lz=self.Lz, Nx=self.Nx, Ny=self.Ny, Nz=self.Nz, r_max=self.r_max,
                                     custom_3d_props=opt, beam_center=self.beam_center, beam_profile=self.beam_profile,
                                     theta_inc_deg=self.theta_inc_deg, phi_inc_deg=self.phi_inc_deg,
-                                    seed=self.seed * 1_000_003 + self.epoch)
+                                    semantics=self.semantics, **stream)
+                self.last_mc = mc
                 A = mc['A_3d']
                 absorbed, closure = float(A.sum()), float(mc['energy_closure'])
             else:
@@ -179,7 +216,7 @@ class OracleEngine:
             P, Pn = p['raw'], np.empty_like(p['raw'])
         for _ in range(self.n_substeps):
             thermal3d_step_explicit(T, Tn, Qth, self.k_grid, self.rho_cp_grid, Nx, Ny, Nz, self.dx, self.dy, self.dz,
-                                    self.dt_sub, self.h_eff, self.t_ambient, True)
+                                    self.dt_sub, self.h_eff, self.t_ambient, True, self.bc_mode)
             apply_latent_heat_plateau(Tn, self.H_acc, self.rho_cp_grid, self.ablated, self.t_abl, Nx, Ny, Nz,
                                       self.dry, self.t_void)
             if self.arrhenius is not None:
@@ -199,6 +236,9 @@ class OracleEngine:
             self.plume['raw'] = P
         np.maximum(self.T_peak, self.T, out=self.T_peak)
         t_th = time.perf_counter() - t1
+        if capture is not None:
+            capture.update(T=self.T.copy(), H_acc=self.H_acc.copy(), chi=self.chi.copy(), dry=self.dry.copy(),
+                           ablated=self.ablated.copy())
         self.t += self.dt_epoch
         self.epoch += 1
         if self.dry_state is None:

@@ -8,17 +8,32 @@ from test_oracle_golden import MC_CASES, _mc_case
 pytestmark = pytest.mark.gpu
 
 
+# The reference's 400k-photon sample of the 45 deg refraction slab (verification_benchmarks.py:131-151)
+# records T = 0.30701 +- 0.00041, 3.4 of its standard errors above the exact value 0.30561 (Fresnel
+# entrance split, Beer-Lambert along the refracted path, no Fresnel at the far face); the FP64
+# oracle with 8e6 photons lands on the exact value. That case is judged against the exact T and A.
+EXACT = {"oblique_v1f": ("oblique45_T", "Transmission", "Absorption")}
+GPU_FACTOR = 10   # GPU photons per reference photon: the combined SE is the reference's x sqrt(1.1)
+
+
 @pytest.mark.parametrize("name", MC_CASES)
 def test_gpu_mc_matches_reference_statistics(gpu, orc, golden, name):
+    """R / A / T / lateral within 3 combined standard errors of the reference's batch statistics."""
     stats = golden("mc_stats.json")[name]
+    an = golden("mc_stats.json")["analytic"]
     kw, nb, npb = _mc_case(name)
     n = nb * npb
-    r = gpu.run_voxel_mc3d(n_photons=n, base_seed=4321, **kw)
+    r = gpu.run_voxel_mc3d(n_photons=GPU_FACTOR * n, base_seed=4321, **kw)
     assert r["engine"] == "gpu"
-    for key, (mean, se) in stats["stats"].items():
-        # deterministic channels (R_spec) differ by FP32 rounding only
-        tol = 3.5 * np.sqrt(2.0) * se + 1e-6
-        assert abs(r["spectro_raw"][key] - mean) <= tol, (key, r["spectro_raw"][key], mean, tol)
+    means = {key: mean for key, (mean, se) in stats["stats"].items()}
+    if name in EXACT:
+        key_an, key_t, key_a = EXACT[name]
+        means[key_t] = an[key_an]
+        means[key_a] = 1.0 - an[key_an] - an["oblique45_Rspec"]
+    for key, (_, se) in stats["stats"].items():
+        # deterministic channels (R_spec, and channels no photon reaches) differ by FP32 rounding only
+        tol = 3.0 * se * np.sqrt(1.0 + 1.0 / GPU_FACTOR) + 1e-6
+        assert abs(r["spectro_raw"][key] - means[key]) <= tol, (key, r["spectro_raw"][key], means[key], tol)
     # FP64 ledger closes to round-off once roulette and truncation are accounted
     assert abs(r["ledger_closure"] - 1.0) < 1e-9
     assert abs(r["energy_closure"] - 1.0) < 0.01
@@ -28,10 +43,11 @@ def test_gpu_mc_matches_reference_statistics(gpu, orc, golden, name):
     if ref.sum() > 0:
         assert np.corrcoef(prof, ref)[0, 1] > 0.995
     # same photon streams in the FP64 oracle: FP32 vs FP64 arithmetic only
+    g = gpu.run_voxel_mc3d(n_photons=n, base_seed=4321, **kw)
     o = orc.run_voxel_mc3d(n_photons=n, seed=4321, **kw)
     for key in stats["stats"]:
-        assert abs(r["spectro_raw"][key] - o["spectro_raw"][key]) < 2e-3, key
-    assert np.allclose(r["A_3d"].sum(), o["A_3d"].sum(), rtol=2e-3)
+        assert abs(g["spectro_raw"][key] - o["spectro_raw"][key]) < 2e-3, key
+    assert np.allclose(g["A_3d"].sum(), o["A_3d"].sum(), rtol=2e-3)
 
 
 def test_gpu_mc_specular_is_exact_fresnel(gpu, golden):
