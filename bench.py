@@ -281,8 +281,7 @@ def ours_main(args):
     from bug_defense_b200 import _lib
     kv = ctypes.c_int(0)
     _lib.call("bd_tune_get", _lib.TUNE_PLUME_KERNEL, ctypes.byref(kv))
-    plume_kernel = {0: "k_plume_step_tma", 1: "k_plume_xm<2>", 2: "k_plume_xm<4>",
-                    3: "k_plume_tb<2>", 4: "k_plume_direct_z"}.get(kv.value, "k_plume_step")
+    plume_kernel = {4: "k_plume_direct_z", 5: "k_plume_resident"}.get(kv.value, "k_plume_step")
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():

@@ -163,6 +163,8 @@ TUNE_MC_BLOCKS_PER_SM = 0
 TUNE_STENCIL_XC = 1
 TUNE_PLUME_XC = 2
 TUNE_PLUME_KERNEL = 3
+PLUME_KERNEL_DIRECT = 4
+PLUME_KERNEL_RESIDENT = 5
 
 CONV_FWD_RELU = 0
 CONV_FWD_UPADD = 1

@@ -18,7 +18,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OUT_DIR = PKG / "_native"
 LIB = OUT_DIR / "libbugdef.so"
-SOURCES = ["abi.cu", "tmap.cu", "mc.cu", "stencil.cu", "phase.cu", "engine.cu", "record.cu", "conv3d.cu", "unet.cu",
+SOURCES = ["abi.cu", "tmap.cu", "mc.cu", "stencil.cu", "plume.cu", "phase.cu", "engine.cu", "record.cu", "conv3d.cu", "unet.cu",
            "selftest.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

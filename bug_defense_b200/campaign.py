@@ -19,6 +19,7 @@ same three spectra (water_mua, melanin_mua, baseline_tissue_mua) from its own ta
 """
 from __future__ import annotations
 
+import ctypes
 import math
 import time
 
@@ -174,15 +175,15 @@ def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=
     """Pick launch shapes by timing them on a throwaway engine of the real workload: `inst` is a
     campaign instance dict or a callable returning an engine with a `laser_power` attribute.
     MC CTAs per SM (photons per thread) are timed by the MC stage of laser-on epochs; x-planes per
-    CTA of the fused substep kernel, the plume kernel and its x-planes (kernel 0) or CTAs per SM
-    (persistent kernels) by the whole epoch with the laser off, when the void domain does not
-    change between trials. Sets the winning values process-wide (bd_tune_set) and returns the
+    CTA of the fused substep kernel, the plume kernel (resident or one launch per step) and the
+    direct plume kernel's x-planes per CTA by the whole epoch with the laser off, when the void
+    domain does not change between trials. Sets the winning values process-wide (bd_tune_set) and returns the
     choices with every trial's time (ms per epoch)."""
     from . import _lib
     cand = dict(candidates or {})
     cand.setdefault(_lib.TUNE_MC_BLOCKS_PER_SM, [2, 4, 6, 8])
     cand.setdefault(_lib.TUNE_STENCIL_XC, [4, 8, 16])
-    cand.setdefault(_lib.TUNE_PLUME_KERNEL, [0, 1, 2, 3, 4])
+    cand.setdefault(_lib.TUNE_PLUME_KERNEL, [_lib.PLUME_KERNEL_DIRECT, _lib.PLUME_KERNEL_RESIDENT])
     cand.setdefault(_lib.TUNE_PLUME_XC, [2, 3, 4, 6])
     stage = {_lib.TUNE_MC_BLOCKS_PER_SM: 0, _lib.TUNE_STENCIL_XC: 1, _lib.TUNE_PLUME_XC: 2, _lib.TUNE_PLUME_KERNEL: 2}
     names = {_lib.TUNE_MC_BLOCKS_PER_SM: "mc_ctas_per_sm", _lib.TUNE_STENCIL_XC: "stencil_xc",
@@ -210,20 +211,32 @@ def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=
 
 
 class Campaign:
-    """Run many instances concurrently: one engine and one CUDA stream per instance, epochs enqueued
-    round-robin with no host synchronisation between them (diagnostics are read every
-    `sync_every` epochs). The laser of instance i is on for its first epochs_on epochs."""
+    """Run many instances together: one engine per instance, epochs enqueued round-robin with no
+    host synchronisation between them (diagnostics are read every `sync_every` epochs). The laser
+    of instance i is on for its first epochs_on epochs.
+
+    With the resident plume kernel (the default) each instance's plume stage occupies every SM, so
+    the instances share one CUDA stream: two resident stages on concurrent streams could each hold
+    part of the GPU while waiting for the rest. With the per-step plume kernel every instance gets
+    its own stream and the instances' stages overlap."""
 
     def __init__(self, instances, device=None, use_graphs: bool = True, log=None):
         import torch
+        from . import _lib
         self.instances = list(instances)
         self.engines = []
         self.streams = []
+        kv = ctypes.c_int(0)
+        _lib.call("bd_tune_get", _lib.TUNE_PLUME_KERNEL, ctypes.byref(kv))
+        self.shared_stream = kv.value == _lib.PLUME_KERNEL_RESIDENT
         t0 = time.perf_counter()
         for inst in self.instances:
             eng = make_engine(inst, device=device, use_graphs=use_graphs)
             self.engines.append(eng)
-            self.streams.append(torch.cuda.Stream(device=eng.dev))
+            if self.shared_stream and self.streams:
+                self.streams.append(self.streams[0])
+            else:
+                self.streams.append(torch.cuda.Stream(device=eng.dev))
             if log:
                 log(f"instance {inst['index']}: {inst['wavelength_nm']:.0f} nm, {inst['power']:.0f} W, "
                     f"pulse {inst['pulse_ms']:.0f} ms")

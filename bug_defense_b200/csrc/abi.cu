@@ -32,7 +32,7 @@ int cuda_status(cudaError_t e, const char* what) {
     return BD_ERR_CUDA;
 }
 
-static std::atomic<int> g_tune[BD_TUNE_COUNT] = {{0}, {8}, {4}, {4}};
+static std::atomic<int> g_tune[BD_TUNE_COUNT] = {{0}, {8}, {4}, {BD_PLUME_KERNEL_RESIDENT}};
 static std::atomic<int> g_tune_gen{0};
 
 int tune_value(int knob) { return g_tune[knob].load(std::memory_order_relaxed); }
@@ -47,7 +47,9 @@ extern "C" int bd_tune_set(int knob, int value) {
     if (knob == BD_TUNE_MC_BLOCKS_PER_SM)
         BD_REQUIRE(value >= 0 && value <= 16, "bd_tune_set: MC CTAs per SM must be 0..16, got %d", value);
     else if (knob == BD_TUNE_PLUME_KERNEL)
-        BD_REQUIRE(value >= 0 && value <= 4, "bd_tune_set: plume kernel must be 0..4, got %d", value);
+        BD_REQUIRE(value == BD_PLUME_KERNEL_DIRECT || value == BD_PLUME_KERNEL_RESIDENT,
+                   "bd_tune_set: plume kernel must be %d (direct) or %d (resident), got %d", BD_PLUME_KERNEL_DIRECT,
+                   BD_PLUME_KERNEL_RESIDENT, value);
     else
         BD_REQUIRE(value >= 1 && value <= 64, "bd_tune_set: x-planes per CTA must be 1..64, got %d", value);
     if (g_tune[knob].exchange(value) != value) g_tune_gen.fetch_add(1);

@@ -22,11 +22,8 @@ int cuda_status(cudaError_t e, const char* what);
 // below 2^62.
 constexpr float kTallyScale = 68719476736.0f;          // 2^36
 constexpr long long kTallyMaxPhotons = 1LL << 26;
-// Plume neighbourhood mask: one byte per voxel, z rows padded to a 16-byte pitch (TMA rows).
+// Plume neighbourhood mask: one byte per voxel, z rows padded to a 16-byte pitch.
 inline int plume_mask_pitch(int nz) { return (nz + 15) / 16 * 16; }
-// After the mask bytes (rounded to 256): the void x-extent of every (z tile, y tile) column of
-// the persistent plume kernel, xmin[kPlumeMaxCols] | xmax[kPlumeMaxCols] | prefix[kPlumeMaxCols + 1].
-constexpr int kPlumeMaxCols = 1024;
 inline size_t plume_mask_only_bytes(int nx, int ny, int nz) {
     return ((size_t)nx * ny * plume_mask_pitch(nz) + 255) / 256 * 256;
 }
@@ -34,15 +31,15 @@ inline size_t plume_mask_only_bytes(int nx, int ny, int nz) {
 // byte per column, then per column the ascending ids of its 4-voxel z groups that hold void
 // (at most (nz + 3) / 4 <= 255 ids; sized for one x plane per chunk).
 constexpr int kPlumeZRows = 16;
-inline size_t plume_zlist_offset(int nx, int ny, int nz) {
-    return plume_mask_only_bytes(nx, ny, nz) + sizeof(int) * (3 * kPlumeMaxCols + 1);
-}
+inline size_t plume_zlist_offset(int nx, int ny, int nz) { return plume_mask_only_bytes(nx, ny, nz); }
 inline size_t plume_zlist_bytes(int nx, int ny, int nz) {
     const size_t cols = (size_t)nx * ((ny + kPlumeZRows - 1) / kPlumeZRows);
     return (cols * (1 + (size_t)(nz + 3) / 4) + 255) / 256 * 256;
 }
+// Then the per-CTA step counters of the resident plume kernel (at most kPlumeMaxTiles CTAs).
+constexpr int kPlumeMaxTiles = 256;
 inline size_t plume_mask_bytes(int nx, int ny, int nz) {
-    return plume_zlist_offset(nx, ny, nz) + plume_zlist_bytes(nx, ny, nz);
+    return plume_zlist_offset(nx, ny, nz) + plume_zlist_bytes(nx, ny, nz) + sizeof(unsigned) * kPlumeMaxTiles;
 }
 
 // Launch-shape knobs (BD_TUNE_*) and the generation counter bumped by every change.

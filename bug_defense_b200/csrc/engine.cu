@@ -292,7 +292,7 @@ extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void*
     const bool laser = power > 0.0f;
     int rc = BD_OK;
     const bool plume = d.n_substeps > 0 && d.has_plume_transport;
-    const bool conc = plume && e->side && !(options & BD_EPOCH_SERIAL_PLUME);
+    const bool conc = plume && e->side && !(options & BD_EPOCH_SERIAL_PLUME) && !plume_resident_active(&d.plume);
     auto plume_stage = [&](cudaStream_t on) -> int {
         return run_stage(e, e->g_plume, &d.plume, sizeof(d.plume), graphs, on, [&](cudaStream_t s) -> int {
             int in_b = 0;

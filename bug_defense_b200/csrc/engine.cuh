@@ -59,6 +59,9 @@ int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, floa
 int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
                  cudaStream_t st, const int* zlimit, int full_first, uint8_t* mask, int* err);
 int plume_policy_steps(const BdPlumeParams* p, int* n_steps, float* dt_step, float* decay_step);
+// true when plume stages of this grid run as one resident launch (its CTAs then occupy every SM for
+// the stage, so the engine runs the stage in line rather than beside MC and the substeps)
+bool plume_resident_active(const BdPlumeParams* p);
 // Per-epoch xz recording (record.cu): inputs of one launch.
 struct RecordArgs {
     int nx, ny, nz, y, k_surface, gap_k0, gap_k1;

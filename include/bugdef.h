@@ -356,14 +356,18 @@ BD_API int bd_engine_record(BdEngine* e, const BdRecordSpec* spec, void* slot, v
 #define BD_TUNE_MC_BLOCKS_PER_SM  0  /* persistent MC grid: 128-thread CTAs per SM, 1..16 (0 = occupancy
                                         limit); photons per thread = n_photons / (grid * 128)          */
 #define BD_TUNE_STENCIL_XC        1  /* x-planes per CTA of the TMA substep kernel, 1..64 (default 8)   */
-#define BD_TUNE_PLUME_XC          2  /* plume kernels 0 and 4: x-planes per CTA; kernels 1-3: CTAs per SM
-                                        (capped by occupancy); 1..64 (default 4)                       */
-#define BD_TUNE_PLUME_KERNEL      3  /* plume step: 0 = one voxel per thread, x chunks per CTA; 1 / 2 =
-                                        persistent, four z voxels per thread marching x, 2 / 4 x-planes
-                                        per copy; 3 = as 1 with two time steps per launch; 4 = a CTA per
-                                        32 x 16 tile marching x planes, no staging, over each tile
-                                        column's live z groups after a stage's first two steps
-                                        (default 4)                                                     */
+#define BD_TUNE_PLUME_XC          2  /* direct plume kernel: x-planes per CTA, 1..64 (default 4)         */
+#define BD_TUNE_PLUME_KERNEL      3  /* plume stage: BD_PLUME_KERNEL_RESIDENT (default) or
+                                        BD_PLUME_KERNEL_DIRECT                                          */
+#define BD_PLUME_KERNEL_DIRECT    4  /* one launch per FTCS step: a CTA per 32 (z) x 16 (y) tile column
+                                        marching x planes over the column's live z groups              */
+#define BD_PLUME_KERNEL_RESIDENT  5  /* one launch per stage: a persistent CTA per column tile (at most
+                                        15 x 20) keeps its tile in shared memory for every step and
+                                        swaps a one-voxel halo with its neighbours through L2; it holds
+                                        every SM for the stage, so stages of engines that run on other
+                                        streams at the same time must use BD_PLUME_KERNEL_DIRECT. Grids
+                                        whose tiles exceed the SMs, or nz % 4 != 0, use the direct
+                                        kernel                                                          */
 #define BD_TUNE_COUNT             4
 BD_API int bd_tune_set(int knob, int value);
 BD_API int bd_tune_get(int knob, int* value);

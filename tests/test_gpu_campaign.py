@@ -34,8 +34,9 @@ def test_knob_validation(gpu, restore_knobs):
         _knob(_lib.TUNE_STENCIL_XC, 0)
     with pytest.raises(ValueError):
         _knob(_lib.TUNE_MC_BLOCKS_PER_SM, 17)
-    with pytest.raises(ValueError):
-        _knob(_lib.TUNE_PLUME_KERNEL, 5)
+    for bad in (0, 3, 6):
+        with pytest.raises(ValueError):
+            _knob(_lib.TUNE_PLUME_KERNEL, bad)
     with pytest.raises(ValueError):
         _knob(7, 1)
 
@@ -63,11 +64,12 @@ def test_launch_shapes_leave_results_bit_identical(gpu, restore_knobs):
 
 
 def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
-    """Every plume kernel gives the same bits: the scalar kernel (several x-chunk lengths), the
-    persistent x-marching kernels (several grid sizes, i.e. run splits) and the direct kernel
-    (several x-chunk lengths), through the context API (full writes on the first steps, ragged y
-    tiles, scattered void, a partly filled last z tile) and through the engine (void z-limit,
-    partly void voxel groups at the crater walls, bulk-void fast path)."""
+    """Every plume kernel gives the same bits: the resident kernel (one launch per stage, tiles
+    kept in shared memory, halos swapped between CTAs; z >= 128 updated from global memory) and the
+    direct kernel (several x-chunk lengths), through the context API (arbitrary values in non-void
+    voxels, ragged y tiles, scattered void, a partly filled last z tile, columns deeper than the
+    shared-memory part) and through the engine (void z-limit, partly void voxel groups at the crater
+    walls, bulk-void fast path)."""
     from bug_defense_b200 import _lib, campaign
     rng = np.random.default_rng(11)
     scattered = rng.uniform(size=(9, 35, 68)) < 0.7
@@ -85,8 +87,7 @@ def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
         C0 = (rng.uniform(0, 1, shape) * vd).astype(np.float32)
         z = np.zeros(shape)
         fields = []
-        for kern, xc in ((0, 4), (0, 2), (1, 4), (1, 1), (2, 2), (2, 1), (1, 3), (3, 2), (3, 1), (4, 2),
-                         (4, 1), (4, 3), (4, 4)):
+        for kern, xc in ((5, 4), (4, 2), (4, 1), (4, 3), (4, 4)):
             _knob(_lib.TUNE_PLUME_KERNEL, kern)
             _knob(_lib.TUNE_PLUME_XC, xc)
             ctx = gpu.MetalAblationContext(*shape, 0.03, 0.025, 0.02, 1e-5, 0.0, 20.0, 100.0, 300.0,
@@ -101,7 +102,7 @@ def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
         assert np.any(fields[0] != C0)
     inst = _small(22)                                  # 2940 nm, 80 W: a crater opens
     runs = []
-    for kern in (0, 1, 2, 3, 4):
+    for kern in (5, 4):
         _knob(_lib.TUNE_PLUME_KERNEL, kern)
         camp = campaign.Campaign([inst])
         camp.run(14, sync_every=14)
@@ -112,12 +113,13 @@ def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
         assert all(np.array_equal(a, b) for a, b in zip(r, runs[0]))
 
 
-def test_concurrent_plume_stage_equals_serial(gpu):
-    """The plume stage runs on its own stream beside MC + substeps by default; within an epoch the
-    stages share no data, so running it after the substeps on one stream gives the same bits. The
-    stage-timing ring stays readable in both modes."""
+def test_concurrent_plume_stage_equals_serial(gpu, restore_knobs):
+    """With the per-step plume kernel the plume stage runs on its own stream beside MC + substeps;
+    within an epoch the stages share no data, so running it after the substeps on one stream gives
+    the same bits. The stage-timing ring stays readable in both modes."""
     import ctypes
     from bug_defense_b200 import _lib, campaign
+    _knob(_lib.TUNE_PLUME_KERNEL, _lib.PLUME_KERNEL_DIRECT)
     inst = _small(22)                                  # 2940 nm, 80 W: a crater opens, plume injected
     runs = []
     for serial in (True, False):
@@ -144,11 +146,13 @@ def _small(index, photons=20_000):
     return dict(inst, n_photons=photons, pulse_ms=12.0)
 
 
-def test_concurrent_campaign_equals_instances_run_alone(gpu, restore_knobs):
-    import torch
-    from bug_defense_b200 import campaign
+@pytest.mark.parametrize("kern", [4, 5], ids=["direct-streams", "resident-one-stream"])
+def test_concurrent_campaign_equals_instances_run_alone(gpu, restore_knobs, kern):
+    from bug_defense_b200 import _lib, campaign
+    _knob(_lib.TUNE_PLUME_KERNEL, kern)
     insts = [_small(i) for i in (1, 10, 23)]           # 532, 1064 and 2940 nm
     camp = campaign.Campaign(insts)
+    assert camp.shared_stream == (kern == _lib.PLUME_KERNEL_RESIDENT)
     camp.run(30, sync_every=10)
     together = [(e.T.copy(), e.ablated.copy(), e.H_acc.copy()) for e in camp.engines]
     for inst, (T, abl, H) in zip(insts, together):
@@ -165,7 +169,7 @@ def test_autotune_sets_the_fastest_candidates(gpu, restore_knobs):
     from bug_defense_b200 import _lib, campaign
     res = campaign.autotune(_small(4), epochs_per_trial=2,
                             candidates={_lib.TUNE_MC_BLOCKS_PER_SM: [2, 4], _lib.TUNE_STENCIL_XC: [4, 8],
-                                        _lib.TUNE_PLUME_KERNEL: [0, 2], _lib.TUNE_PLUME_XC: [2, 4]})
+                                        _lib.TUNE_PLUME_KERNEL: [4, 5], _lib.TUNE_PLUME_XC: [2, 4]})
     for name, knob in (("mc_ctas_per_sm", _lib.TUNE_MC_BLOCKS_PER_SM), ("stencil_xc", _lib.TUNE_STENCIL_XC),
                        ("plume_kernel", _lib.TUNE_PLUME_KERNEL), ("plume_xc", _lib.TUNE_PLUME_XC)):
         trials = res["trials"][name]
