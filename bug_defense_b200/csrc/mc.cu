@@ -23,6 +23,7 @@
 #include <stdlib.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 namespace bd {
@@ -531,17 +532,20 @@ int mc_launch(const BdMcParams* p, const float* props, const uint8_t* flags, flo
               double* latz, double* ledger, unsigned long long* queue, double* partials, int max_blocks,
               int sm_count, cudaStream_t st, const long long* offset_dev, unsigned long long* tally64) {
     McDev d = mc_dev_params(p);
-    static int per_sm[2] = {0, 0};
+    // resident 128-thread CTAs per SM of each kernel variant: computed once, shared by host threads
+    static std::atomic<int> per_sm[2] = {{0}, {0}};
     const int ax = p->launch_axis == 0 ? 0 : 1;
-    if (per_sm[ax] == 0) {
+    int occ = per_sm[ax].load(std::memory_order_relaxed);
+    if (occ == 0) {
         int nb = 0;
         if (ax == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_mc_trace<2>, 128, 0);
         else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_mc_trace<0>, 128, 0);
-        per_sm[ax] = std::max(1, std::min(nb, 16));
+        occ = std::max(1, std::min(nb, 16));
         cudaGetLastError();
+        per_sm[ax].store(occ, std::memory_order_relaxed);
     }
     const int want = tune_value(BD_TUNE_MC_BLOCKS_PER_SM);
-    const int use_sm = want > 0 ? std::min(want, per_sm[ax]) : per_sm[ax];
+    const int use_sm = want > 0 ? std::min(want, occ) : occ;
     int blocks = (int)std::min<long long>((p->n_photons + 127) / 128, (long long)sm_count * use_sm);
     blocks = std::max(1, std::min(blocks, max_blocks));
     BD_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st));
@@ -643,7 +647,9 @@ extern "C" int bd_mc_trace_noalloc(const BdMcParams* p, const float* props, cons
     int sms = 0;
     {
         // set-up once per device, with that device current: the array's name is only a host-side
-        // stand-in, the kernel must be given the device address of this device's copy
+        // stand-in, the kernel must be given the device address of this device's copy. The address
+        // is cached for the life of the device's primary context: do not use this entry point across
+        // a cudaDeviceReset of that device.
         std::lock_guard<std::mutex> lock(g_mc_noalloc_mu);
         if (g_mc_noalloc_ptr[dev] == nullptr) {
             void* ptr = nullptr;
@@ -656,16 +662,8 @@ extern "C" int bd_mc_trace_noalloc(const BdMcParams* p, const float* props, cons
         base = g_mc_noalloc_ptr[dev];
         sms = g_mc_noalloc_sms[dev];
     }
-    // the grid this launch needs (persistent, occupancy-sized) must fit the static ledger rows
-    int per_sm = 0;
-    if (p->launch_axis == 0) BD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mc_trace<2>, 128, 0));
-    else BD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mc_trace<0>, 128, 0));
-    per_sm = std::max(1, std::min(per_sm, 16));
-    const long long need = std::max(1LL, std::min<long long>((p->n_photons + 127) / 128, (long long)sms * per_sm));
-    if (need > MC_NOALLOC_MAX_BLOCKS)
-        return fail(BD_ERR_INVALID_ARG,
-                    "bd_mc_trace_noalloc: this launch needs %lld blocks but the static scratch holds %d "
-                    "(use bd_mc_trace)", need, MC_NOALLOC_MAX_BLOCKS);
+    // the kernel is persistent (a photon queue), so any photon count runs on at most
+    // MC_NOALLOC_MAX_BLOCKS blocks: mc_launch caps the grid at the static ledger rows
     unsigned long long* queue = static_cast<unsigned long long*>(base);
     double* partials = reinterpret_cast<double*>(static_cast<unsigned char*>(base) + MC_NOALLOC_QUEUE_BYTES);
     // mc_launch zeroes the queue counter and the ledger rows it uses before the kernel runs

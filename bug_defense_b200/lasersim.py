@@ -191,29 +191,61 @@ def build_model(layers, wavelength_nm, voxel_um, eval_layer=fallback_layer_optic
     }
 
 
-def _regions(ranges, nz_air):
-    """Slice ranges of the air gap, the core (hemolymph, else the middle soft layer) and the ventral
-    shell (beetle_sim.py:183-198)."""
-    kinds = [r[2] for r in ranges]
-    first_air = next((i for i, kd in enumerate(kinds) if kd == 'air'), None)
-    soft = [i for i, kd in enumerate(kinds) if kd == 'boils']
-    last_soft = soft[-1] if soft else None
-    hemo = next((i for i, r in enumerate(ranges) if r[3] == 'hemolymph'), None)
-    core = hemo if hemo is not None else (soft[len(soft) // 2] if soft else len(ranges) // 2)
-    if last_soft is not None and last_soft < len(ranges) - 1:
-        ventral = (ranges[last_soft][1], ranges[-1][1])
+def layer_regions(ranges, nz_air):
+    """Slice bands the frames summarise (the bookkeeping of beetle_sim.py:183-198): the first air layer
+    (the air gap), the core (the hemolymph layer, else the middle one of the boiling soft layers,
+    else the middle layer), the ventral shell (every slice below the last boiling layer, or the last
+    layer when a boiling layer is last) and the dorsal surface slice. `ranges` holds
+    (k0, k1, kind, name) per layer, top to bottom."""
+    span = lambda r: (r[0], r[1])
+    gap = next((span(r) for r in ranges if r[2] == 'air'), None)
+    boiling = [i for i, r in enumerate(ranges) if r[2] == 'boils']
+    first_of = {}
+    for i, r in enumerate(ranges):
+        first_of.setdefault(r[3], i)
+    if 'hemolymph' in first_of:
+        core = first_of['hemolymph']
+    elif boiling:
+        core = boiling[len(boiling) // 2]
     else:
-        ventral = (ranges[-1][0], ranges[-1][1])
-    return {'air_gap': (ranges[first_air][0], ranges[first_air][1]) if first_air is not None else None,
-            'core': (ranges[core][0], ranges[core][1]), 'ventral': ventral, 'surface': nz_air}
+        core = len(ranges) // 2
+    last = len(ranges) - 1
+    ventral = (ranges[boiling[-1]][1], ranges[last][1]) if boiling and boiling[-1] < last else span(ranges[last])
+    return {'air_gap': gap, 'core': span(ranges[core]), 'ventral': ventral, 'surface': nz_air}
 
 
-def _encode(arr, dtype):
-    return base64.b64encode(np.ascontiguousarray(arr, dtype=dtype).tobytes()).decode('ascii')
+def b64_slice(arr, dtype) -> str:
+    """A 2-D slice as base64 of its C-ordered bytes in `dtype` (the frame payload the UI decodes)."""
+    return base64.b64encode(memoryview(np.require(arr, dtype=dtype, requirements='C'))).decode('ascii')
 
 
-def _stride(n, limit=120):
-    return max(1, int(math.ceil(n / limit)))
+def decimation(n: int, cap: int = 120) -> int:
+    """Sampling step along an axis of n voxels that keeps at most `cap` samples in a frame."""
+    return max(1, -(-n // cap))
+
+
+def aim_beam(theta_deg: float, body_mm: float, air_mm: float):
+    """Beam centre on the grid's top face for which the incident axis, tilted by theta in x, passes
+    the lateral centre half-way down the body (below `air_mm` of air above the dorsal surface)."""
+    return LX / 2.0 - math.tan(math.radians(theta_deg)) * (air_mm + 0.5 * body_mm), LY / 2.0
+
+
+def _setup_payload(geo, reg, xs, zs_um, voxel_um, photons, laser_echo):
+    """The 'setup' event of beetle_sim.run: sampled axes, grid, reference lines and layer table."""
+    d, nz_air = geo['dz'], geo['nz_air']
+    depth_um = lambda k: round((k - nz_air) * d * 1000.0, 1)
+    gap = reg['air_gap']
+    nx, ny, nz = geo['shape']
+    return {
+        'nx': len(xs), 'nz': len(zs_um),
+        'x_mm': [round(v, 4) for v in xs], 'z_um': [round(v, 2) for v in zs_um],
+        'grid': f'{nx}x{ny}x{nz}', 'voxel_um': voxel_um, 'photons': photons,
+        'lines_um': {'surface': 0.0, 'air_gap_start': depth_um(gap[0]) if gap else None,
+                     'air_gap_end': depth_um(gap[1]) if gap else None, 'ventral_shell': depth_um(reg['ventral'][0])},
+        'layers': [{'name': r[3], 'kind': r[2], 'z_start_um': depth_um(r[0]), 'z_end_um': depth_um(r[1])}
+                   for r in geo['ranges']],
+        'laser': laser_echo,
+    }
 
 
 def run(layers, laser, frame_ms_active=2.0, frame_ms_cooling=10.0, eval_layer=fallback_layer_optics, device=None):
@@ -234,11 +266,8 @@ def run(layers, laser, frame_ms_active=2.0, frame_ms_cooling=10.0, eval_layer=fa
     d = geo['dz']
     nz_air = geo['nz_air']
     l_body = (nz - nz_air) * d
-    reg = _regions(geo['ranges'], nz_air)
-    # aim so the beam axis crosses the lateral centre half-way through the body
-    tan_t = math.tan(math.radians(theta))
-    x_dorsal = LX / 2.0 - tan_t * l_body / 2.0
-    beam_center = (x_dorsal - nz_air * d * tan_t, LY / 2.0)
+    reg = layer_regions(geo['ranges'], nz_air)
+    beam_center = aim_beam(theta, l_body, nz_air * d)
 
     engine = CoupledAblationEngine(
         optical_props=geo['optical'], k_grid=geo['k_grid'], rho_cp_grid=geo['rho_cp_grid'],
@@ -250,30 +279,17 @@ def run(layers, laser, frame_ms_active=2.0, frame_ms_cooling=10.0, eval_layer=fa
         air_gap_range=reg['air_gap'], wavelength_nm=wl, device=device)
 
     mid_y = ny // 2
-    sx, sz = _stride(nx), _stride(nz)
+    sx, sz = decimation(nx), decimation(nz)
     grid_x = (np.arange(nx) + 0.5) * d - LX / 2.0
     grid_z = ((np.arange(nz) + 0.5) - nz_air) * d * 1000.0      # um, 0 = dorsal surface
     tissue = ~geo['is_air'][::sx, mid_y, ::sz]
     n_tissue = max(1, int(np.sum(tissue)))
-    um = lambda k: round((k - nz_air) * d * 1000.0, 1)
     c0, c1 = reg['core']
     v0, v1 = reg['ventral']
     rec = Recorder(engine, y=mid_y, k_surface=nz_air, bands=((nz_air, nz_air), (c0, c1), (v0, v1)), ring=1)
-
-    yield {'event': 'setup', 'data': {
-        'nx': len(grid_x[::sx]), 'nz': len(grid_z[::sz]),
-        'x_mm': [round(v, 4) for v in grid_x[::sx]], 'z_um': [round(v, 2) for v in grid_z[::sz]],
-        'grid': f'{nx}x{ny}x{nz}', 'voxel_um': voxel_um, 'photons': photons,
-        'lines_um': {
-            'surface': 0.0,
-            'air_gap_start': um(reg['air_gap'][0]) if reg['air_gap'] else None,
-            'air_gap_end': um(reg['air_gap'][1]) if reg['air_gap'] else None,
-            'ventral_shell': um(reg['ventral'][0]),
-        },
-        'layers': [{'name': r[3], 'kind': r[2], 'z_start_um': um(r[0]), 'z_end_um': um(r[1])} for r in geo['ranges']],
-        'laser': {'wavelength_nm': wl, 'power_w': power, 'spot_dia_mm': spot, 'theta_deg': theta,
-                  'pulse_ms': pulse_s * 1000.0, 'duration_ms': total_s * 1000.0, 'plume': plume_on},
-    }}
+    echo = {'wavelength_nm': wl, 'power_w': power, 'spot_dia_mm': spot, 'theta_deg': theta,
+            'pulse_ms': pulse_s * 1000.0, 'duration_ms': total_s * 1000.0, 'plume': plume_on}
+    yield {'event': 'setup', 'data': _setup_payload(geo, reg, grid_x[::sx], grid_z[::sz], voxel_um, photons, echo)}
 
     n_epochs = int(round(total_s / DT_EPOCH))
     e_inc = e_abs = e_refl = e_trans = 0.0
@@ -311,8 +327,8 @@ def run(layers, laser, frame_ms_active=2.0, frame_ms_cooling=10.0, eval_layer=fa
         yield {'event': 'frame', 'data': {
             't_ms': round(t_ms, 2), 'laser_on': bool(on), 'progress': round((ep + 1) / n_epochs, 4),
             'eta_s': round(elapsed / (ep + 1) * (n_epochs - ep - 1), 1),
-            'Q': _encode(np.maximum(Q[::sx, ::sz], 1e-4).T, '<f4'), 'T': _encode(T[::sx, ::sz].T, '<f4'),
-            'plume': _encode(plume[::sx, ::sz].T, '<f4'), 'phase': _encode(ph_s.T, 'u1'),
+            'Q': b64_slice(np.maximum(Q[::sx, ::sz], 1e-4).T, '<f4'), 'T': b64_slice(T[::sx, ::sz].T, '<f4'),
+            'plume': b64_slice(plume[::sx, ::sz].T, '<f4'), 'phase': b64_slice(ph_s.T, 'u1'),
             'transmission_pct': round(100.0 * math.exp(-float(row['plume_tau'])), 2),
             'core_peak': round(float(core.max()) if core.size else T_AMBIENT, 2),
             'core_mean': round(float(core.mean()) if core.size else T_AMBIENT, 2),

@@ -186,8 +186,9 @@ BD_API int bd_mc_trace(BdMcContext* ctx, const BdMcParams* p, const float* props
  * owns all device memory through its own pool. Its scratch (photon-queue counter + one FP64
  * ledger row per block, 256 B + 2048 x 16 doubles = 256.25 KiB) is a static device array that
  * every GPU loading this library holds until the process exits. The first call on a device
- * looks up that device's copy of the array, so make it before any timing-critical phase.
- * Launches needing more than 2048 blocks are rejected with BD_ERR_INVALID_ARG. Every call
+ * looks up that device's copy of the array (cached until a cudaDeviceReset of that device, after
+ * which this entry point must not be used), so make it before any timing-critical phase. The
+ * kernel is persistent, so any photon count runs on a grid capped at 2048 blocks. Every call
  * shares the array: calls that overlap on the GPU (other streams, other host threads on the
  * same device) race and must be serialised by the caller. Its absorbed map is summed with FP32
  * atomics (bd_mc_trace sums exactly in 64-bit fixed point, which needs per-voxel scratch): the

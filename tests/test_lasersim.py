@@ -45,5 +45,5 @@ def test_build_model_matches_reference(gold, voxel):
     np.testing.assert_array_equal(geo["initial_ablated"][0, 0, :], gold[f"{tag}_ablated"])
     assert [list(r) for r in geo["ranges"]] == json.loads(str(gold[f"{tag}_ranges"]))
     reg = json.loads(str(gold[f"{tag}_regions"]))
-    got = ls._regions(geo["ranges"], geo["nz_air"])
+    got = ls.layer_regions(geo["ranges"], geo["nz_air"])
     assert json.loads(json.dumps(got)) == reg

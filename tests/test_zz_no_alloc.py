@@ -30,22 +30,25 @@ def _outputs(torch, shape, dev):
 
 
 def test_noalloc_entry_point_matches_allocating_one_on_two_calls(gpu):
+    """Two calls in a row, the first with more photons (a larger grid: more ledger rows of the
+    shared array in use) than the second, each against bd_mc_trace with the same parameters."""
     import torch
     from bug_defense_b200 import _lib, voxel_mc
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     shape, props, p = _setup(torch, voxel_mc, dev)
-    A0, L0, z0, led0 = _outputs(torch, shape, dev)
-    voxel_mc.trace(p, props, A0, L0, z0, led0)   # existing entry point, bd_mc_trace
-    torch.cuda.synchronize()
     lib = _lib.load()
-    for call in range(2):
+    for n_photons in (200_000, 40_000):
+        p.n_photons = n_photons
+        A0, L0, z0, led0 = _outputs(torch, shape, dev)
+        voxel_mc.trace(p, props, A0, L0, z0, led0)   # existing entry point, bd_mc_trace
         A1, L1, z1, led1 = _outputs(torch, shape, dev)
         rc = lib.bd_mc_trace_noalloc(ctypes.byref(p), _lib.ptr(props), None, _lib.ptr(A1), _lib.ptr(L1),
                                      _lib.ptr(z1), _lib.ptr(led1), _lib.stream_ptr())
         _lib.check(rc, "bd_mc_trace_noalloc")
         torch.cuda.synchronize()
         a, b = led0.cpu().numpy(), led1.cpu().numpy()
+        assert a[0] == n_photons
         # same photon streams: counts identical, FP64 weights equal up to summation order
         np.testing.assert_array_equal(a[[0, 10, 11, 12]], b[[0, 10, 11, 12]])
         np.testing.assert_allclose(b, a, rtol=1e-12, atol=1e-9)
