@@ -26,15 +26,22 @@ HEAD_BYTES = 256
 class Recorder:
     """Record epochs of a CoupledAblationEngine.
 
-    y: xz slice (default mid-y); ix: centreline column (default mid-x); k_surface: first slice below
-    the ambient air (crater depth origin); bands: three (k0, k1) z ranges for peak_T_dorsal,
-    peak_T_core, peak_T_ventral; ring: pinned slots in flight."""
+    y: xz slice (default mid-y); ix: centreline column (default mid-x), or beam_ix: the centreline's
+    x index in every slice (a tilted beam axis, the production runner's sampling line); k_surface:
+    first slice below the ambient air (crater depth origin, and the origin of the record's grid_z);
+    bands: three (k0, k1) z ranges for peak_T_dorsal, peak_T_core, peak_T_ventral; ring: pinned slots
+    in flight."""
 
-    def __init__(self, eng, y=None, ix=None, k_surface=0, bands=((0, 0), (0, 0), (0, 0)), ring: int = 16):
+    def __init__(self, eng, y=None, ix=None, k_surface=0, bands=((0, 0), (0, 0), (0, 0)), ring: int = 16,
+                 beam_ix=None):
         self.eng = eng
         self.nx, self.ny, self.nz = eng.shape
         self.y = self.ny // 2 if y is None else int(y)
         self.ix = self.nx // 2 if ix is None else int(ix)
+        if beam_ix is None:
+            self.line = np.full(self.nz, self.ix, dtype=np.int64)
+        else:
+            self.line = np.clip(np.asarray(beam_ix, dtype=np.int64).reshape(self.nz), 0, self.nx - 1)
         self.k_surface = int(k_surface)
         self.bands = [tuple(int(v) for v in b) for b in bands]
         self.slot_bytes = int(_lib.load().bd_record_slot_bytes(self.nx, self.nz))
@@ -113,11 +120,12 @@ class Recorder:
         eps = sorted(self.rows)
         R = [self.rows[e] for e in eps]
         dz = self.eng.dz
+        zs = np.arange(self.nz)
         return dict(
             times=np.array([r["time_s"] for r in R]),
-            centerline_T=np.array([r["T"][self.ix] for r in R], dtype=np.float32),
-            centerline_Q=np.array([r["Q"][self.ix] for r in R], dtype=np.float32),
-            centerline_phase=np.array([r["phase"][self.ix] for r in R], dtype=np.uint8),
+            centerline_T=np.array([r["T"][self.line, zs] for r in R], dtype=np.float32),
+            centerline_Q=np.array([r["Q"][self.line, zs] for r in R], dtype=np.float32),
+            centerline_phase=np.array([r["phase"][self.line, zs] for r in R], dtype=np.uint8),
             xz_T=np.array([r["T"] for r in R], dtype=np.float32),
             xz_Q=np.array([r["Q"] for r in R], dtype=np.float32),
             xz_phase=np.array([r["phase"] for r in R], dtype=np.uint8),
@@ -129,11 +137,26 @@ class Recorder:
             crater_depths_mm=np.array([r["depth_voxels"] * dz for r in R]),
         )
 
-    def save_npz(self, path, **meta):
-        """np.savez_compressed with the keys of the runner's record (run_highres_knowledge_suite.py:
-        330-367): the per-epoch series, the grids and the caller's metadata (wavelength_nm, power_w...)."""
+    def record_arrays(self, arrays=None, gap_k0=None, **meta) -> dict:
+        """The runner's whole record (run_highres_knowledge_suite.py:330-367): the per-epoch series, the
+        grids (grid_z from -k_surface dz at the top of the grid to the bottom, 0 = dorsal surface), the
+        time of the first ablated voxel in the mid-y slice just above the air gap (t_perforation_s,
+        slice gap_k0 - 1, default the engine's air gap) and of the first core-band peak at or above
+        99.5 C (t_core_boil_s), None when never, the grid constants and the caller's metadata."""
         eng = self.eng
-        a = self.finish()
-        np.savez_compressed(path, **a, grid_x=np.linspace(0, eng.Lx, eng.Nx), grid_y=np.linspace(0, eng.Ly, eng.Ny),
-                            grid_z=np.linspace(0, eng.Lz, eng.Nz), NX=eng.Nx, NY=eng.Ny, NZ=eng.Nz, DX=eng.dx,
-                            DY=eng.dy, DZ=eng.dz, dt_epoch=eng.dt_epoch, **meta)
+        a = self.finish() if arrays is None else arrays
+        k0 = gap_k0 if gap_k0 is not None else (self.gap[0] if self.gap[1] > self.gap[0] else None)
+        t = np.asarray(a["times"])
+        perf = np.flatnonzero((a["xz_phase"][:, :, k0 - 1] == 3).any(axis=1)) if k0 else np.zeros(0, int)
+        boil = np.flatnonzero(np.asarray(a["peak_T_core"]) >= 99.5)
+        top = self.k_surface * eng.dz
+        return dict(a, grid_x=np.linspace(0, eng.Lx, eng.Nx), grid_y=np.linspace(0, eng.Ly, eng.Ny),
+                    grid_z=np.linspace(-top, eng.Nz * eng.dz - top, eng.Nz),
+                    t_perforation_s=float(t[perf[0]]) if perf.size else None,
+                    t_core_boil_s=float(t[boil[0]]) if boil.size else None,
+                    NX=eng.Nx, NY=eng.Ny, NZ=eng.Nz, DX=eng.dx, DY=eng.dy, DZ=eng.dz, dt_epoch=eng.dt_epoch, **meta)
+
+    def save_npz(self, path, **meta):
+        """np.savez_compressed of record_arrays(): the keys of the runner's record, with the caller's
+        metadata (wavelength_nm, power_w, ...)."""
+        np.savez_compressed(path, **self.record_arrays(**meta))
