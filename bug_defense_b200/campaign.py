@@ -215,7 +215,7 @@ class Campaign:
     host synchronisation between them (diagnostics are read every `sync_every` epochs). The laser
     of instance i is on for its first epochs_on epochs.
 
-    With the resident plume kernel (the default) each instance's plume stage occupies every SM, so
+    With the resident plume kernel (BD_PLUME_KERNEL_RESIDENT) each instance's plume stage occupies every SM, so
     the instances share one CUDA stream: two resident stages on concurrent streams could each hold
     part of the GPU while waiting for the rest. With the per-step plume kernel every instance gets
     its own stream and the instances' stages overlap."""

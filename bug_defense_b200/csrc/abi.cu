@@ -32,7 +32,7 @@ int cuda_status(cudaError_t e, const char* what) {
     return BD_ERR_CUDA;
 }
 
-static std::atomic<int> g_tune[BD_TUNE_COUNT] = {{0}, {8}, {4}, {BD_PLUME_KERNEL_RESIDENT}};
+static std::atomic<int> g_tune[BD_TUNE_COUNT] = {{0}, {8}, {4}, {BD_PLUME_KERNEL_DIRECT}};
 static std::atomic<int> g_tune_gen{0};
 
 int tune_value(int knob) { return g_tune[knob].load(std::memory_order_relaxed); }

@@ -2,13 +2,12 @@
 // diffusion with upwind drift, zero flux at solid walls (the neighbour value is replaced by the
 // centre), Dirichlet 0 on the outer walls, clamped at 0, optional first-order decay.
 //
-// Kernels (all evaluate the same per-voxel expression, ftcs(), so they are bit-identical):
-//   k_plume_resident  default (BD_PLUME_KERNEL_RESIDENT): one persistent CTA per column tile of at
-//                     most 15 x 20 keeps its tile of the field in shared memory for every step of a
-//                     stage and swaps a one-voxel halo with its four neighbours through L2 per step
-//   k_plume_direct_z  (BD_PLUME_KERNEL_DIRECT, and the fallback when the tiles exceed the SMs): one
-//                     launch per step, a CTA per 32 (z) x 16 (y) tile column marching x planes over
-//                     the column's live z groups
+// Kernels (all evaluate the same per-voxel expression, ftcs1 / ftcs4, so they are bit-identical):
+//   k_plume_resident  (BD_PLUME_KERNEL_RESIDENT): one persistent CTA per column tile of at most
+//                     15 x 20 keeps its tile of the field in shared memory for every step of a stage
+//                     and swaps a one-voxel halo with its four neighbours through L2 per step
+//   k_plume_direct_z  default (BD_PLUME_KERNEL_DIRECT): one launch per step, a CTA per 32 (z) x 16 (y)
+//                     tile column marching x planes over the column's live z groups
 //   k_plume_step      any grid (nz % 4 != 0): one voxel per thread
 // Layout: C-order (nx, ny, nz), z fastest; the neighbourhood of every voxel is one mask byte.
 #include "common.cuh"
@@ -62,61 +61,92 @@ struct PlumeConst {
     float vz_over_dz, dtp, decay;
 };
 
-// Stencil weights of one step: C' = decay * (w0 C + wx (C-x + C+x) + wy (C-y + C+y) + wb C-z + wt C+z),
-// the FTCS step of plume.py:46-80 with the upwind drift term folded into wt and w0.
-struct PlumeW {
-    float w0, wx, wy, wb, wt, decay;
+// Weights of one step. plume.py:46-80 updates a void voxel as
+//   C' = decay * (C + dt (D_xy (lap_x + lap_y) + D_z lap_z - v (C - C_{+z}) / dz)),
+// with a solid neighbour's value replaced by the centre's (zero flux). Every kernel keeps solid
+// voxels at 0, so that replacement is the same as adding the solid neighbour's weight to the centre:
+//   C' = decay * (w0eff C + wx (C_-x + C_+x) + wy (C_-y + C_+y) + wb C_-z + wt C_+z),
+// w0eff = w0 + the weights of the solid neighbours, one of 64 values picked by the six neighbour
+// bits of the voxel's mask byte. The table is built once per stage on the host, in float32, in a
+// fixed order, so every kernel applies the same weights.
+struct PlumeTab {
+    float wx, wy, wb, wt, decay;
+    int decays;          // decay != 1 (a factor of exactly 1 is skipped: x * 1 == x)
+    float w0eff[64];
 };
 
-__host__ __device__ inline PlumeW plume_weights(const PlumeConst& c) {
-    PlumeW k;
-    k.wx = c.dtp * c.dxy_x; k.wy = c.dtp * c.dxy_y; k.wb = c.dtp * c.dz_z;
-    k.wt = k.wb + c.dtp * c.vz_over_dz;
-    k.w0 = 1.0f - 2.0f * (k.wx + k.wy + k.wb) - c.dtp * c.vz_over_dz;
-    k.decay = c.decay;
-    return k;
+static PlumeTab make_plume_tab(const PlumeConst& c) {
+    PlumeTab t;
+    t.wx = c.dtp * c.dxy_x;
+    t.wy = c.dtp * c.dxy_y;
+    t.wb = c.dtp * c.dz_z;
+    const float adv = c.dtp * c.vz_over_dz;
+    t.wt = t.wb + adv;
+    const float w0 = 1.0f - 2.0f * (t.wx + t.wy + t.wb) - adv;
+    for (int b = 0; b < 64; ++b) {
+        float e = w0;
+        if (!(b & 0x01)) e += t.wx;
+        if (!(b & 0x02)) e += t.wx;
+        if (!(b & 0x04)) e += t.wy;
+        if (!(b & 0x08)) e += t.wy;
+        if (!(b & 0x10)) e += t.wb;
+        if (!(b & 0x20)) e += t.wt;
+        t.w0eff[b] = e;
+    }
+    t.decay = c.decay;
+    t.decays = c.decay != 1.0f;
+    return t;
 }
 
-// One voxel's FTCS update from its neighbours and mask byte, the expression of every plume kernel.
-// The rounding of each operation is spelled out so that every kernel (and every inlining context)
-// produces the same bits. FAST: the caller has established that, if the voxel is updated, all six
-// neighbours are void.
-template <bool FAST>
-__device__ __forceinline__ float ftcs(float c0, float w, float e, float s, float n, float b, float t, unsigned m,
-                                      const PlumeW& k) {
-    if (!FAST) {
-        w = (m & 0x01) ? w : c0;
-        e = (m & 0x02) ? e : c0;
-        s = (m & 0x04) ? s : c0;
-        n = (m & 0x08) ? n : c0;
-        b = (m & 0x10) ? b : c0;
-        t = (m & 0x20) ? t : c0;
-    }
-    float a = __fmul_rn(k.w0, c0);
+// One voxel (the scalar form; the packed form below performs the same operations per component).
+__device__ __forceinline__ float ftcs1(float c0, float w, float e, float s, float n, float b, float t, unsigned m,
+                                       const PlumeTab& k) {
+    float a = __fmul_rn(k.w0eff[m & 0x3Fu], c0);
     a = __fmaf_rn(k.wx, __fadd_rn(w, e), a);
     a = __fmaf_rn(k.wy, __fadd_rn(s, n), a);
     a = __fmaf_rn(k.wb, b, a);
     a = __fmaf_rn(k.wt, t, a);
-    const float u = fmaxf(__fmul_rn(a, k.decay), 0.0f);
-    return (m & BD_PM_UPDATE) ? u : 0.0f;
-}
-
-// true when every voxel of the byte set `m` that is updated has all six neighbours void
-__device__ __forceinline__ bool all_interior(unsigned m) {
-    const unsigned upd = (m >> 7) & 0x01010101u;
-    return (m & (upd * 0x3Fu)) == upd * 0x3Fu;
+    if (k.decays) a = __fmul_rn(a, k.decay);
+    return (m & BD_PM_UPDATE) ? fmaxf(a, 0.0f) : 0.0f;
 }
 
 // Four consecutive z voxels (one float4 and their four mask bytes); zb / zt: the voxels below and
-// above the group. FAST as in ftcs.
-template <bool FAST>
+// above the group. Pairs of voxels go through the packed FP32x2 operations of sm_100 (each lane
+// rounded as the scalar operation), which halves the arithmetic instructions.
+// w0eff: the table of effective centre weights, wherever the caller keeps it (shared memory in the
+// resident kernel, whose lanes index it divergently).
 __device__ __forceinline__ float4 ftcs4(float4 c, float4 w, float4 e, float4 s, float4 n, float zb, float zt,
-                                       unsigned m, const PlumeW& k) {
+                                        unsigned m, const PlumeTab& k, const float* w0eff) {
+    const float2 wx = make_float2(k.wx, k.wx), wy = make_float2(k.wy, k.wy);
+    const float2 wb = make_float2(k.wb, k.wb), wt = make_float2(k.wt, k.wt);
+    // a group whose four voxels have six void neighbours each (the bulk of the domain) needs no lookup
+    float2 wa, wc;
+    if ((m & 0x3F3F3F3Fu) == 0x3F3F3F3Fu) {
+        wa = wc = make_float2(w0eff[0x3F], w0eff[0x3F]);
+    } else {
+        wa = make_float2(w0eff[m & 0x3Fu], w0eff[(m >> 8) & 0x3Fu]);
+        wc = make_float2(w0eff[(m >> 16) & 0x3Fu], w0eff[(m >> 24) & 0x3Fu]);
+    }
+    float2 a = __fmul2_rn(wa, make_float2(c.x, c.y));
+    float2 b = __fmul2_rn(wc, make_float2(c.z, c.w));
+    a = __ffma2_rn(wx, __fadd2_rn(make_float2(w.x, w.y), make_float2(e.x, e.y)), a);
+    b = __ffma2_rn(wx, __fadd2_rn(make_float2(w.z, w.w), make_float2(e.z, e.w)), b);
+    a = __ffma2_rn(wy, __fadd2_rn(make_float2(s.x, s.y), make_float2(n.x, n.y)), a);
+    b = __ffma2_rn(wy, __fadd2_rn(make_float2(s.z, s.w), make_float2(n.z, n.w)), b);
+    a = __ffma2_rn(wb, make_float2(zb, c.x), a);
+    b = __ffma2_rn(wb, make_float2(c.y, c.z), b);
+    a = __ffma2_rn(wt, make_float2(c.y, c.z), a);
+    b = __ffma2_rn(wt, make_float2(c.w, zt), b);
+    if (k.decays) {
+        const float2 d = make_float2(k.decay, k.decay);
+        a = __fmul2_rn(a, d);
+        b = __fmul2_rn(b, d);
+    }
     float4 v;
-    v.x = ftcs<FAST>(c.x, w.x, e.x, s.x, n.x, zb, c.y, m & 0xffu, k);
-    v.y = ftcs<FAST>(c.y, w.y, e.y, s.y, n.y, c.x, c.z, (m >> 8) & 0xffu, k);
-    v.z = ftcs<FAST>(c.z, w.z, e.z, s.z, n.z, c.y, c.w, (m >> 16) & 0xffu, k);
-    v.w = ftcs<FAST>(c.w, w.w, e.w, s.w, n.w, c.z, zt, m >> 24, k);
+    v.x = (m & 0x00000080u) ? fmaxf(a.x, 0.0f) : 0.0f;
+    v.y = (m & 0x00008000u) ? fmaxf(a.y, 0.0f) : 0.0f;
+    v.z = (m & 0x00800000u) ? fmaxf(b.x, 0.0f) : 0.0f;
+    v.w = (m & 0x80000000u) ? fmaxf(b.y, 0.0f) : 0.0f;
     return v;
 }
 
@@ -126,32 +156,48 @@ __device__ __forceinline__ unsigned zkeep_mask(int zl, int k) {
     return nk >= 4 ? 0xffffffffu : (nk <= 0 ? 0u : (0xffffffffu >> (8 * (4 - nk))));
 }
 
+// Non-void voxels of a field set to 0 (the context API's input may hold anything there): afterwards
+// both ping-pong buffers satisfy the invariant every step relies on.
+__global__ void k_plume_clear(float* __restrict__ Ca, float* __restrict__ Cb, const uint8_t* __restrict__ M, int nx,
+                              int ny, int nz, int mz) {
+    const long long n = (long long)nx * ny * nz;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long col = i / nz;
+        const int k = (int)(i - col * nz);
+        if (!(M[col * mz + k] & BD_PM_VOID)) {
+            Ca[i] = 0.0f;
+            Cb[i] = 0.0f;
+        }
+    }
+}
+
 // ---- k_plume_step: any grid ----------------------------------------------------------------
 // One FTCS step. CTA (y tile, x plane); a thread owns the voxels k = tx, tx+32, ... < zlim of one
-// (x, y) column (zlim = *zlimit when given, every void voxel lies above it, else nz). Non-void voxels
-// are written (as 0) only when full_write is set: the engine keeps them 0 in both ping-pong buffers.
-__global__ void __launch_bounds__(PM_TZ * PM_TY) k_plume_step(int nx, int ny, int nz, int mz, PlumeConst c,
+// (x, y) column (zlim = *zlimit when given, every void voxel lies above it, else nz); only void
+// voxels are written (solid voxels stay 0).
+__global__ void __launch_bounds__(PM_TZ * PM_TY) k_plume_step(int nx, int ny, int nz, int mz,
+                                                              const __grid_constant__ PlumeTab k,
                                                               const float* __restrict__ C, float* __restrict__ Cn,
                                                               const uint8_t* __restrict__ M,
-                                                              const int* __restrict__ zlimit, int full_write) {
+                                                              const int* __restrict__ zlimit) {
     const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
     const int j = blockIdx.x * PM_TY + threadIdx.y;
     const int i = blockIdx.y;
     if (j >= ny) return;
-    const PlumeW kw = plume_weights(c);
     const int plane = ny * nz;
     const int col = i * plane + j * nz;
     const size_t mcol = ((size_t)i * ny + j) * mz;
-    for (int k = threadIdx.x; k < zl; k += PM_TZ) {
-        const int idx = col + k;
-        const unsigned m = __ldg(&M[mcol + k]);
+    for (int z = threadIdx.x; z < zl; z += PM_TZ) {
+        const int idx = col + z;
+        const unsigned m = __ldg(&M[mcol + z]);
+        if (!(m & BD_PM_VOID)) continue;
         if (!(m & BD_PM_UPDATE)) {
-            if ((m & BD_PM_VOID) || full_write) Cn[idx] = 0.0f;
+            Cn[idx] = 0.0f;
             continue;
         }
         // an updated voxel is never on an outer wall: all six neighbours exist
-        Cn[idx] = ftcs<false>(__ldg(&C[idx]), __ldg(&C[idx - plane]), __ldg(&C[idx + plane]), __ldg(&C[idx - nz]),
-                              __ldg(&C[idx + nz]), __ldg(&C[idx - 1]), __ldg(&C[idx + 1]), m, kw);
+        Cn[idx] = ftcs1(__ldg(&C[idx]), __ldg(&C[idx - plane]), __ldg(&C[idx + plane]), __ldg(&C[idx - nz]),
+                        __ldg(&C[idx + nz]), __ldg(&C[idx - 1]), __ldg(&C[idx + 1]), m, k);
     }
 }
 
@@ -162,32 +208,44 @@ __global__ void __launch_bounds__(PM_TZ * PM_TY) k_plume_step(int nx, int ny, in
 // centre plane's y neighbours from the (L2-resident) field beside the plane's mask bytes (one
 // 32-bit load): one L2 round trip per plane, at the price of loads a tissue plane does not need. The
 // z neighbours come from the neighbouring lanes by shuffle (the tile's edge lanes load them).
-// Latency is hidden by the many independent CTAs of a step. Warp-uniform paths: no void (nothing to
-// do), every updated voxel with six void neighbours (no selects), the general path. Needs nz % 4 == 0
-// and 16-byte aligned fields.
+// Latency is hidden by the many independent CTAs of a step. Only void voxels are written. Needs
+// nz % 4 == 0 and 16-byte aligned fields.
 constexpr int PL_BZ = 32;
 constexpr int PD_BY = 16;  // rows per CTA (8 * PD_BY threads)
 static_assert(PD_BY == kPlumeZRows, "z-list columns follow the direct kernel's y tiles");
 
+__device__ __forceinline__ void store_void(float* dst, float4 v, unsigned vd) {
+    if (vd == 0x40404040u) {
+        *reinterpret_cast<float4*>(dst) = v;
+    } else {
+        if (vd & 0x00000040u) dst[0] = v.x;
+        if (vd & 0x00004000u) dst[1] = v.y;
+        if (vd & 0x00400000u) dst[2] = v.z;
+        if (vd & 0x40000000u) dst[3] = v.w;
+    }
+}
+
 __global__ void __launch_bounds__(8 * PD_BY) k_plume_direct(const float* __restrict__ C, float* __restrict__ Cn,
                                                             const uint8_t* __restrict__ M, int nx, int ny, int nz,
-                                                            int mz, int xc, PlumeConst c,
-                                                            const int* __restrict__ zlimit, int full_write) {
+                                                            int mz, int xc, const __grid_constant__ PlumeTab k,
+                                                            const int* __restrict__ zlimit) {
+    __shared__ float w0s[64];
+    if (threadIdx.x < 64) w0s[threadIdx.x] = k.w0eff[threadIdx.x];
+    __syncthreads();
     const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
     const int k0 = blockIdx.x * PL_BZ;
     const int ib = blockIdx.z * xc, ie = min(nx, ib + xc);
     if (k0 >= zl || ib >= ie) return;  // uniform over the CTA
     const int zg = threadIdx.x & 7;
-    const int j = blockIdx.y * PD_BY + (threadIdx.x >> 3), k = k0 + 4 * zg;
-    const bool act = zl - k > 0 && j < ny;
-    const bool in = j < ny && k < nz;
-    const unsigned zkeep = zkeep_mask(zl, k);
+    const int j = blockIdx.y * PD_BY + (threadIdx.x >> 3), z = k0 + 4 * zg;
+    const bool act = zl - z > 0 && j < ny;
+    const bool in = j < ny && z < nz;
+    const unsigned zkeep = zkeep_mask(zl, z);
     const size_t plane = (size_t)ny * nz;
     const size_t mplane = (size_t)ny * mz;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    size_t idx = ((size_t)ib * ny + j) * nz + k;
-    const uint8_t* mp = M + ((size_t)ib * ny + j) * mz + k;
-    const PlumeW kw = plume_weights(c);
+    size_t idx = ((size_t)ib * ny + j) * nz + z;
+    const uint8_t* mp = M + ((size_t)ib * ny + j) * mz + z;
     float4 cw = in && ib > 0 ? __ldg(reinterpret_cast<const float4*>(C + idx - plane)) : z4;
     float4 cc = in ? __ldg(reinterpret_cast<const float4*>(C + idx)) : z4;
     for (int i = ib; i < ie; ++i, idx += plane, mp += mplane) {
@@ -196,28 +254,16 @@ __global__ void __launch_bounds__(8 * PD_BY) k_plume_direct(const float* __restr
         const float4 cs = in && j > 0 ? __ldg(reinterpret_cast<const float4*>(C + idx - nz)) : z4;
         const float4 cn = in && j + 1 < ny ? __ldg(reinterpret_cast<const float4*>(C + idx + nz)) : z4;
         float eb = 0.0f, et = 0.0f;
-        if (zg == 0 && in && k > 0) eb = __ldg(C + idx - 1);
-        if (zg == 7 && in && k + 4 < nz) et = __ldg(C + idx + 4);
+        if (zg == 0 && in && z > 0) eb = __ldg(C + idx - 1);
+        if (zg == 7 && in && z + 4 < nz) et = __ldg(C + idx + 4);
         const unsigned vd = mr & 0x40404040u;
-        if (__any_sync(0xffffffffu, act && (vd || full_write))) {
+        if (__any_sync(0xffffffffu, act && vd)) {
             float zb = __shfl_up_sync(0xffffffffu, cc.w, 1, 8);
             float zt = __shfl_down_sync(0xffffffffu, cc.x, 1, 8);
             if (zg == 0) zb = eb;
             if (zg == 7) zt = et;
-            const float4 v = __all_sync(0xffffffffu, all_interior(mr) || !act)
-                                 ? ftcs4<true>(cc, cw, ce, cs, cn, zb, zt, mr, kw)
-                                 : ftcs4<false>(cc, cw, ce, cs, cn, zb, zt, mr, kw);
-            if (act && (vd || full_write)) {
-                float* dst = Cn + idx;
-                if (full_write || vd == 0x40404040u) {
-                    *reinterpret_cast<float4*>(dst) = v;
-                } else {
-                    if (vd & 0x00000040u) dst[0] = v.x;
-                    if (vd & 0x00004000u) dst[1] = v.y;
-                    if (vd & 0x00400000u) dst[2] = v.z;
-                    if (vd & 0x40000000u) dst[3] = v.w;
-                }
-            }
+            const float4 v = ftcs4(cc, cw, ce, cs, cn, zb, zt, mr, k, w0s);
+            if (act && vd) store_void(Cn + idx, v, vd);
         }
         cw = cc;
         cc = ce;
@@ -273,9 +319,13 @@ __global__ void __launch_bounds__(256) k_plume_zlist(const uint8_t* __restrict__
 // never written.
 __global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_z(const float* __restrict__ C, float* __restrict__ Cn,
                                                                  const uint8_t* __restrict__ M, int nx, int ny,
-                                                                 int nz, int mz, int xc, PlumeConst c,
+                                                                 int nz, int mz, int xc,
+                                                                 const __grid_constant__ PlumeTab k,
                                                                  const int* __restrict__ zlimit,
                                                                  const uint8_t* __restrict__ zlist) {
+    __shared__ float w0s[64];
+    if (threadIdx.x < 64) w0s[threadIdx.x] = k.w0eff[threadIdx.x];
+    __syncthreads();
     const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
     const int G = (nz + 3) / 4;
     const int n_cols = gridDim.y * gridDim.z;
@@ -290,16 +340,15 @@ __global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_z(const float* __
     const int gn = __shfl_down_sync(0xffffffffu, g, 1, 8);
     const bool zb_lane = zg > 0 && gp == g - 1;  // the -z neighbour is the previous lane's last voxel
     const bool zt_lane = zg < 7 && gn == g + 1;  // the +z neighbour is the next lane's first voxel
-    const int j = blockIdx.y * PD_BY + (threadIdx.x >> 3), k = 4 * max(g, 0);
-    const bool act = g >= 0 && zl - k > 0 && j < ny;
-    const bool in = g >= 0 && j < ny && k < nz;
-    const unsigned zkeep = zkeep_mask(zl, k);
+    const int j = blockIdx.y * PD_BY + (threadIdx.x >> 3), z = 4 * max(g, 0);
+    const bool act = g >= 0 && zl - z > 0 && j < ny;
+    const bool in = g >= 0 && j < ny && z < nz;
+    const unsigned zkeep = zkeep_mask(zl, z);
     const size_t plane = (size_t)ny * nz;
     const size_t mplane = (size_t)ny * mz;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    size_t idx = ((size_t)ib * ny + j) * nz + k;
-    const uint8_t* mp = M + ((size_t)ib * ny + j) * mz + k;
-    const PlumeW kw = plume_weights(c);
+    size_t idx = ((size_t)ib * ny + j) * nz + z;
+    const uint8_t* mp = M + ((size_t)ib * ny + j) * mz + z;
     float4 cw = in && ib > 0 ? __ldg(reinterpret_cast<const float4*>(C + idx - plane)) : z4;
     float4 cc = in ? __ldg(reinterpret_cast<const float4*>(C + idx)) : z4;
     for (int i = ib; i < ie; ++i, idx += plane, mp += mplane) {
@@ -308,28 +357,16 @@ __global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_z(const float* __
         const float4 cs = in && j > 0 ? __ldg(reinterpret_cast<const float4*>(C + idx - nz)) : z4;
         const float4 cn = in && j + 1 < ny ? __ldg(reinterpret_cast<const float4*>(C + idx + nz)) : z4;
         float eb = 0.0f, et = 0.0f;
-        if (!zb_lane && in && k > 0) eb = __ldg(C + idx - 1);
-        if (!zt_lane && in && k + 4 < nz) et = __ldg(C + idx + 4);
+        if (!zb_lane && in && z > 0) eb = __ldg(C + idx - 1);
+        if (!zt_lane && in && z + 4 < nz) et = __ldg(C + idx + 4);
         const unsigned vd = mr & 0x40404040u;
         if (__any_sync(0xffffffffu, act && vd)) {
             float zb = __shfl_up_sync(0xffffffffu, cc.w, 1, 8);
             float zt = __shfl_down_sync(0xffffffffu, cc.x, 1, 8);
             if (!zb_lane) zb = eb;
             if (!zt_lane) zt = et;
-            const float4 v = __all_sync(0xffffffffu, all_interior(mr) || !act)
-                                 ? ftcs4<true>(cc, cw, ce, cs, cn, zb, zt, mr, kw)
-                                 : ftcs4<false>(cc, cw, ce, cs, cn, zb, zt, mr, kw);
-            if (act && vd) {
-                float* dst = Cn + idx;
-                if (vd == 0x40404040u) {
-                    *reinterpret_cast<float4*>(dst) = v;
-                } else {
-                    if (vd & 0x00000040u) dst[0] = v.x;
-                    if (vd & 0x00004000u) dst[1] = v.y;
-                    if (vd & 0x00400000u) dst[2] = v.z;
-                    if (vd & 0x40000000u) dst[3] = v.w;
-                }
-            }
+            const float4 v = ftcs4(cc, cw, ce, cs, cn, zb, zt, mr, k, w0s);
+            if (act && vd) store_void(Cn + idx, v, vd);
         }
         cw = cc;
         cc = ce;
@@ -340,25 +377,35 @@ __global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_z(const float* __
 // The (x, y) columns are cut into tiles_x x tiles_y tiles of at most RS_TX x RS_TY columns, one CTA
 // per tile, all resident at once (cooperative launch, one CTA per SM). A CTA copies its tile of the
 // field, with a one-column ring of its neighbours' columns, into shared memory for z < min(zl, RS_Z)
-// (zl = void z-limit) and keeps it there for every step of the stage. A step marches the tile's x
-// planes; a thread owns RS_PPT (y, 4-voxel z group) positions of a plane and keeps the x-1 / x float4
-// of each in registers, reads the x+1 / y+-1 / z+-1 neighbours from shared memory, and, after a CTA
-// barrier (every read of the plane done), writes the plane's new values in place. The new values of
-// the tile's boundary columns are also stored to the global ping-pong buffer of the next state;
-// after the step a release flag tells the four neighbours, each CTA waits (acquire) for its
-// neighbours' flags and copies their boundary columns into its ring. Neighbours are therefore never
-// more than one step apart, and two global buffers suffice: a buffer is rewritten two steps after it
-// was read. Voxels at z >= RS_Z (craters deeper than the shared-memory column) are updated straight
-// from and to the global ping-pong buffers by the same CTA in the same plane pass. The final state
-// of the tile is written to buffer (n_steps & 1). Every wait is bounded in time: on a timeout the
-// CTA raises *err and stops (the stage result is then undefined and the engine reports
-// BD_ERR_TIMEOUT).
-constexpr int RS_TX = 15, RS_TY = 20, RS_Z = 128, RS_THREADS = 320, RS_PPT = 2;
-constexpr int RS_G = RS_Z / 4;  // float4 groups per shared-memory column
-static_assert(RS_TY * RS_G <= RS_PPT * RS_THREADS, "every shared-memory position of a plane needs a thread slot");
-constexpr size_t RS_C_BYTES = (size_t)(RS_TX + 2) * (RS_TY + 2) * RS_Z * sizeof(float);
+// (zl = void z-limit) and keeps it there for every step of the stage. Warp w owns rows
+// [RS_R w, RS_R w + RS_R) of the tile and lane l the 4-voxel z group l, so the z neighbours of a
+// group come from the neighbouring lanes by shuffle and the y neighbours inside a warp's rows from
+// its own registers; only the rows just above and below the warp's block are read from shared
+// memory. A step marches the tile's x planes keeping the x-1 / x float4 of every row in registers;
+// after a CTA barrier (every read of the plane done) the plane's new values are written in place.
+// The new values of the tile's boundary columns are also stored to the global ping-pong buffer of
+// the next state; after the step a release flag tells the four neighbours, each CTA waits (acquire)
+// for its neighbours' flags and copies their boundary columns into its ring. Neighbours are
+// therefore never more than one step apart, and two global buffers suffice: a buffer is rewritten two
+// steps after it was read. Voxels at z >= RS_Z (craters deeper than the shared-memory column) are
+// updated straight from and to the global ping-pong buffers by the same CTA in the same plane pass.
+// The final state of the tile is written to buffer (n_steps & 1). Every wait is bounded in time: on
+// a timeout the CTA raises *err and stops (the stage result is then undefined and the engine
+// reports BD_ERR_TIMEOUT).
+#ifndef BD_PLUME_RS_R
+#define BD_PLUME_RS_R 2
+#endif
+constexpr int RS_TX = 15, RS_TY = 20, RS_Z = 128, RS_R = BD_PLUME_RS_R;
+constexpr int RS_G = RS_Z / 4;                    // float4 groups per shared-memory column (= warp lanes)
+constexpr int RS_WARPS = (RS_TY + RS_R - 1) / RS_R;
+constexpr int RS_THREADS = 32 * RS_WARPS;
+static_assert(RS_G == 32, "a warp's lanes are the z groups of a shared-memory column");
+// shared field: (RS_TX + 2) planes x (RS_TY + 2) rows of columns, plus RS_R + 1 spare columns read
+// (never used) by the last warp when the tile has fewer rows than the warps cover
+constexpr size_t RS_C_BYTES = ((size_t)(RS_TX + 2) * (RS_TY + 2) + RS_R + 1) * RS_Z * sizeof(float);
 constexpr size_t RS_M_BYTES = (size_t)RS_TX * RS_TY * RS_Z;
-constexpr size_t RS_SMEM = RS_C_BYTES + RS_M_BYTES + 16;
+constexpr size_t RS_SMEM = RS_C_BYTES + RS_M_BYTES + 64 * sizeof(float) + 16;
+constexpr int RS_BATCH = 8;   // independent L2 loads a thread issues before storing them to shared memory
 constexpr long long RS_TIMEOUT_NS = 500000000LL;  // 0.5 s per wait (a step takes microseconds)
 
 struct ResidentArgs {
@@ -370,7 +417,7 @@ struct ResidentArgs {
     int* err;
     int nx, ny, nz, mz;
     int tiles_x, tiles_y, n_steps;
-    PlumeConst c;
+    PlumeTab k;
 };
 
 __device__ __forceinline__ long long global_ns() {
@@ -389,13 +436,12 @@ __device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-__global__ void __launch_bounds__(RS_THREADS, 1) k_plume_resident(ResidentArgs a) {
+__global__ void __launch_bounds__(RS_THREADS, 1) k_plume_resident(const __grid_constant__ ResidentArgs a) {
     extern __shared__ __align__(16) unsigned char rs_smem[];
-    float* Cs = reinterpret_cast<float*>(rs_smem);
     float4* Cs4 = reinterpret_cast<float4*>(rs_smem);
-    const unsigned* Ms4 = reinterpret_cast<const unsigned*>(rs_smem + RS_C_BYTES);
-    unsigned* Ms4w = reinterpret_cast<unsigned*>(rs_smem + RS_C_BYTES);
-    volatile int* s_fail = reinterpret_cast<volatile int*>(rs_smem + RS_C_BYTES + RS_M_BYTES);
+    unsigned* Ms4 = reinterpret_cast<unsigned*>(rs_smem + RS_C_BYTES);
+    float* w0s = reinterpret_cast<float*>(rs_smem + RS_C_BYTES + RS_M_BYTES);
+    volatile int* s_fail = reinterpret_cast<volatile int*>(rs_smem + RS_C_BYTES + RS_M_BYTES + 64 * sizeof(float));
 
     const int nx = a.nx, ny = a.ny, nz = a.nz;
     const int zl = a.zlimit ? min(max(*a.zlimit, 0), nz) : nz;
@@ -409,16 +455,16 @@ __global__ void __launch_bounds__(RS_THREADS, 1) k_plume_resident(ResidentArgs a
     const int Gs = (zs + 3) / 4;       // their float4 groups
     const int Gg = (zl + 3) / 4 - Gs;  // groups per column kept in global memory (zl > RS_Z)
     const int row = ty + 2;            // ring rows per plane
+    const int PS = row * RS_G;         // float4 stride of a plane
     const size_t plane = (size_t)ny * nz;
-    const int tid = threadIdx.x;
-    const PlumeW kw = plume_weights(a.c);
-    auto cidx = [&](int lx, int ly) { return (lx * row + ly) * RS_G; };  // float4 index of a smem column
-    auto gidx = [&](int x, int y, int k) { return ((size_t)x * ny + y) * nz + k; };
+    const int tid = threadIdx.x, lane = tid & 31, yb = (tid >> 5) * RS_R;
+    auto gidx = [&](int x, int y, int z) { return ((size_t)x * ny + y) * nz + z; };
 
     // zero the shared field (ring columns outside the grid and z >= zl stay 0), then load the tile
     // and its ring (corners excluded) at the stage's start state, and the tile's mask bytes
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int i = tid; i < (tx + 2) * row * RS_G; i += RS_THREADS) Cs4[i] = z4;
+    for (int i = tid; i < (int)(RS_C_BYTES / 16); i += RS_THREADS) Cs4[i] = z4;
+    if (tid < 64) w0s[tid] = a.k.w0eff[tid];
     if (tid == 0) *s_fail = 0;
     __syncthreads();
     for (int i = tid; i < (tx + 2) * row * Gs; i += RS_THREADS) {
@@ -426,96 +472,89 @@ __global__ void __launch_bounds__(RS_THREADS, 1) k_plume_resident(ResidentArgs a
         const int x = x0 + lx - 1, y = y0 + ly - 1;
         const bool corner = (lx == 0 || lx == tx + 1) && (ly == 0 || ly == ty + 1);
         if (corner || x < 0 || x >= nx || y < 0 || y >= ny) continue;
-        Cs4[cidx(lx, ly) + g] = __ldcg(reinterpret_cast<const float4*>(a.buf0 + gidx(x, y, 4 * g)));
+        Cs4[col * RS_G + g] = __ldcg(reinterpret_cast<const float4*>(a.buf0 + gidx(x, y, 4 * g)));
     }
     for (int i = tid; i < tx * ty * Gs; i += RS_THREADS) {
         const int g = i % Gs, col = i / Gs, y = col % ty, px = col / ty;
         const unsigned m =
             __ldg(reinterpret_cast<const unsigned*>(a.M + ((size_t)(x0 + px) * ny + y0 + y) * a.mz + 4 * g));
-        Ms4w[(px * ty + y) * RS_G + g] = m & zkeep_mask(zl, 4 * g);
+        Ms4[(px * ty + y) * RS_G + g] = m & zkeep_mask(zl, 4 * g);
     }
     __syncthreads();
 
-    int py[RS_PPT], pg[RS_PPT];
-    bool pv[RS_PPT];
+    // this thread: rows yb .. yb + RS_R - 1 (those below ty are real), z group `lane`
+    bool rv[RS_R];
 #pragma unroll
-    for (int q = 0; q < RS_PPT; ++q) {
-        const int p = tid + q * RS_THREADS;
-        pv[q] = p < ty * Gs;
-        py[q] = pv[q] ? p / Gs : 0;
-        pg[q] = pv[q] ? p % Gs : 0;
-    }
-    float4 cw[RS_PPT], cc[RS_PPT];
+    for (int r = 0; r < RS_R; ++r) rv[r] = yb + r < ty && lane < Gs;
+    const int base = (yb + 1) * RS_G + lane;           // float4 index of (plane 0, row yb, lane)
+    float4 cw[RS_R], cc[RS_R];
 #pragma unroll
-    for (int q = 0; q < RS_PPT; ++q) {
-        cw[q] = pv[q] ? Cs4[cidx(0, py[q] + 1) + pg[q]] : z4;
-        cc[q] = pv[q] ? Cs4[cidx(1, py[q] + 1) + pg[q]] : z4;
+    for (int r = 0; r < RS_R; ++r) {
+        cw[r] = Cs4[base + r * RS_G];
+        cc[r] = Cs4[base + PS + r * RS_G];
     }
+    const bool top_from_global = Gg > 0 && lane == RS_G - 1;
 
     bool failed = false;
     for (int t = 0; t < a.n_steps; ++t) {
         const float* gcur = (t & 1) ? a.buf1 : a.buf0;
         float* gnxt = (t & 1) ? a.buf0 : a.buf1;
         for (int px = 0; px < tx; ++px) {
-            const int lx = px + 1, x = x0 + px;
-            float4 v[RS_PPT], ce[RS_PPT];
-            unsigned mm[RS_PPT];
-            bool fast = true;
+            const int pb = base + (px + 1) * PS;   // this thread's first row on the centre plane
+            const int x = x0 + px;
+            float4 ce[RS_R], v[RS_R];
+            unsigned m[RS_R];
 #pragma unroll
-            for (int q = 0; q < RS_PPT; ++q) {
-                mm[q] = pv[q] ? Ms4[(px * ty + py[q]) * RS_G + pg[q]] : 0u;
-                fast = fast && (!pv[q] || all_interior(mm[q]));
+            for (int r = 0; r < RS_R; ++r) {
+                ce[r] = Cs4[pb + PS + r * RS_G];
+                m[r] = rv[r] ? Ms4[(px * ty + yb + r) * RS_G + lane] : 0u;
             }
-            fast = __all_sync(0xffffffffu, fast);
+            const float4 s_edge = Cs4[pb - RS_G];            // row yb - 1 (a ring row for the first block)
+            const float4 n_edge = Cs4[pb + RS_R * RS_G];     // row yb + RS_R (the ring row after the last)
 #pragma unroll
-            for (int q = 0; q < RS_PPT; ++q) {
-                v[q] = z4;
-                ce[q] = z4;
-                if (!pv[q]) continue;
-                const int c0 = cidx(lx, py[q] + 1);
-                ce[q] = Cs4[cidx(lx + 1, py[q] + 1) + pg[q]];
-                const float4 cs = Cs4[cidx(lx, py[q]) + pg[q]];
-                const float4 cn = Cs4[cidx(lx, py[q] + 2) + pg[q]];
-                const int k = 4 * pg[q];
-                const float zb = k > 0 ? Cs[c0 * 4 + k - 1] : 0.0f;
-                float zt = 0.0f;
-                if (k + 4 < RS_Z) zt = Cs[c0 * 4 + k + 4];
-                else if (Gg > 0) zt = __ldcg(gcur + gidx(x, y0 + py[q], RS_Z));
-                v[q] = fast ? ftcs4<true>(cc[q], cw[q], ce[q], cs, cn, zb, zt, mm[q], kw)
-                            : ftcs4<false>(cc[q], cw[q], ce[q], cs, cn, zb, zt, mm[q], kw);
+            for (int r = 0; r < RS_R; ++r) {
+                float zb = __shfl_up_sync(0xffffffffu, cc[r].w, 1);
+                float zt = __shfl_down_sync(0xffffffffu, cc[r].x, 1);
+                if (lane == 0) zb = 0.0f;                    // z = 0 is a wall: never updated
+                if (lane == RS_G - 1) zt = top_from_global ? __ldcg(gcur + gidx(x, y0 + yb + r, RS_Z)) : 0.0f;
+                const float4 s = r == 0 ? s_edge : cc[r - 1];
+                const float4 n = r == RS_R - 1 ? n_edge : cc[r + 1];
+                v[r] = ftcs4(cc[r], cw[r], ce[r], s, n, zb, zt, m[r], a.k, w0s);
             }
             // columns deeper than the shared-memory part: from and to the global buffers
             for (int p = tid; p < ty * Gg; p += RS_THREADS) {
-                const int y = p / Gg, k = 4 * (Gs + p % Gg), yy = y0 + y;
-                const size_t idx = gidx(x, yy, k);
-                const unsigned m = __ldg(reinterpret_cast<const unsigned*>(a.M + ((size_t)x * ny + yy) * a.mz + k)) &
-                                   zkeep_mask(zl, k);
+                const int y = p / Gg, z = 4 * (Gs + p % Gg), yy = y0 + y;
+                const size_t idx = gidx(x, yy, z);
+                const unsigned mg = __ldg(reinterpret_cast<const unsigned*>(a.M + ((size_t)x * ny + yy) * a.mz + z)) &
+                                    zkeep_mask(zl, z);
                 const float4 c = __ldcg(reinterpret_cast<const float4*>(gcur + idx));
                 const float4 w = x > 0 ? __ldcg(reinterpret_cast<const float4*>(gcur + idx - plane)) : z4;
                 const float4 e = x + 1 < nx ? __ldcg(reinterpret_cast<const float4*>(gcur + idx + plane)) : z4;
                 const float4 s = yy > 0 ? __ldcg(reinterpret_cast<const float4*>(gcur + idx - nz)) : z4;
                 const float4 n = yy + 1 < ny ? __ldcg(reinterpret_cast<const float4*>(gcur + idx + nz)) : z4;
-                const float zb = k == RS_Z ? Cs[cidx(lx, y + 1) * 4 + RS_Z - 1] : __ldcg(gcur + idx - 1);
-                const float zt = k + 4 < nz ? __ldcg(gcur + idx + 4) : 0.0f;
-                *reinterpret_cast<float4*>(gnxt + idx) = ftcs4<false>(c, w, e, s, n, zb, zt, m, kw);
+                const float zb = z == RS_Z ? Cs4[(px + 1) * PS + (y + 1) * RS_G + RS_G - 1].w  // smem z = RS_Z - 1
+                                           : __ldcg(gcur + idx - 1);
+                const float zt = z + 4 < nz ? __ldcg(gcur + idx + 4) : 0.0f;
+                const unsigned vd = mg & 0x40404040u;
+                if (vd) store_void(gnxt + idx, ftcs4(c, w, e, s, n, zb, zt, mg, a.k, w0s), vd);
             }
             __syncthreads();  // every read of plane px (and of its neighbours' old values) is done
             const bool xedge = px == 0 || px == tx - 1;
 #pragma unroll
-            for (int q = 0; q < RS_PPT; ++q) {
-                if (!pv[q]) continue;
-                Cs4[cidx(lx, py[q] + 1) + pg[q]] = v[q];
-                if (xedge || py[q] == 0 || py[q] == ty - 1)
-                    *reinterpret_cast<float4*>(gnxt + gidx(x, y0 + py[q], 4 * pg[q])) = v[q];
-                cw[q] = cc[q];
-                cc[q] = ce[q];
+            for (int r = 0; r < RS_R; ++r) {
+                if (rv[r]) {
+                    Cs4[pb + r * RS_G] = v[r];
+                    if (xedge || yb + r == 0 || yb + r == ty - 1)
+                        *reinterpret_cast<float4*>(gnxt + gidx(x, y0 + yb + r, 4 * lane)) = v[r];
+                }
+                cw[r] = cc[r];
+                cc[r] = ce[r];
             }
         }
         __syncthreads();  // the step's boundary stores of every thread are issued
-        if (tid == 0) {
-            __threadfence();
-            st_release_gpu(a.flags + b, (unsigned)(t + 1));
-        }
+        // the barrier orders every thread's boundary stores before thread 0's release (a release at gpu
+        // scope is cumulative over the writes thread 0 has observed through the barrier)
+        if (tid == 0) st_release_gpu(a.flags + b, (unsigned)(t + 1));
         if (t + 1 == a.n_steps) break;
         if (tid < 4) {
             const int nbx = bx + (tid == 0 ? -1 : tid == 1 ? 1 : 0), nby = by + (tid == 2 ? -1 : tid == 3 ? 1 : 0);
@@ -529,7 +568,6 @@ __global__ void __launch_bounds__(RS_THREADS, 1) k_plume_resident(ResidentArgs a
                         break;
                     }
                 }
-                __threadfence();
             }
         }
         __syncthreads();
@@ -537,28 +575,44 @@ __global__ void __launch_bounds__(RS_THREADS, 1) k_plume_resident(ResidentArgs a
             failed = true;
             break;
         }
-        // the neighbours' boundary columns at the new state into the ring
+        // the neighbours' boundary columns at the new state into the ring: RS_BATCH loads in flight
+        // per thread before their shared-memory stores
         const int nring = (2 * ty + 2 * tx) * Gs;
-        for (int i = tid; i < nring; i += RS_THREADS) {
-            const int g = i % Gs, r = i / Gs;
-            int lx, ly;
-            if (r < 2 * ty) {
-                lx = (r < ty) ? 0 : tx + 1;
-                ly = (r % ty) + 1;
-            } else {
-                const int r2 = r - 2 * ty;
-                ly = (r2 < tx) ? 0 : ty + 1;
-                lx = (r2 % tx) + 1;
+        for (int i0 = tid; i0 < nring; i0 += RS_BATCH * RS_THREADS) {
+            float4 val[RS_BATCH];
+            int dst[RS_BATCH];
+#pragma unroll
+            for (int q = 0; q < RS_BATCH; ++q) {
+                const int i = i0 + q * RS_THREADS;
+                dst[q] = -1;
+                val[q] = z4;
+                if (i < nring) {
+                    const int g = i % Gs, r = i / Gs;
+                    int lx, ly;
+                    if (r < 2 * ty) {
+                        lx = (r < ty) ? 0 : tx + 1;
+                        ly = (r % ty) + 1;
+                    } else {
+                        const int r2 = r - 2 * ty;
+                        ly = (r2 < tx) ? 0 : ty + 1;
+                        lx = (r2 % tx) + 1;
+                    }
+                    const int x = x0 + lx - 1, y = y0 + ly - 1;
+                    if (x >= 0 && x < nx && y >= 0 && y < ny) {
+                        dst[q] = (lx * row + ly) * RS_G + g;
+                        val[q] = __ldcg(reinterpret_cast<const float4*>(gnxt + gidx(x, y, 4 * g)));
+                    }
+                }
             }
-            const int x = x0 + lx - 1, y = y0 + ly - 1;
-            if (x < 0 || x >= nx || y < 0 || y >= ny) continue;
-            Cs4[cidx(lx, ly) + g] = __ldcg(reinterpret_cast<const float4*>(gnxt + gidx(x, y, 4 * g)));
+#pragma unroll
+            for (int q = 0; q < RS_BATCH; ++q)
+                if (dst[q] >= 0) Cs4[dst[q]] = val[q];
         }
         __syncthreads();
 #pragma unroll
-        for (int q = 0; q < RS_PPT; ++q) {
-            cw[q] = pv[q] ? Cs4[cidx(0, py[q] + 1) + pg[q]] : z4;
-            cc[q] = pv[q] ? Cs4[cidx(1, py[q] + 1) + pg[q]] : z4;
+        for (int r = 0; r < RS_R; ++r) {
+            cw[r] = Cs4[base + r * RS_G];
+            cc[r] = Cs4[base + PS + r * RS_G];
         }
     }
     if (failed) return;
@@ -566,7 +620,7 @@ __global__ void __launch_bounds__(RS_THREADS, 1) k_plume_resident(ResidentArgs a
     float* out = (a.n_steps & 1) ? a.buf1 : a.buf0;
     for (int i = tid; i < tx * ty * Gs; i += RS_THREADS) {
         const int g = i % Gs, col = i / Gs, y = col % ty, px = col / ty;
-        *reinterpret_cast<float4*>(out + gidx(x0 + px, y0 + y, 4 * g)) = Cs4[cidx(px + 1, y + 1) + g];
+        *reinterpret_cast<float4*>(out + gidx(x0 + px, y0 + y, 4 * g)) = Cs4[((px + 1) * row + y + 1) * RS_G + g];
     }
 }
 
@@ -639,7 +693,8 @@ int plume_policy_steps(const BdPlumeParams* p, int* n_steps, float* dt_step, flo
 
 // A plume stage: n_substeps x (steps per substep) FTCS steps on the ping-pong pair (Ca, Cb), the
 // field in Ca on entry. *in_b = 1 when the result ends in Cb. With full_first (the context API, whose
-// non-void voxels may hold anything) the mask covers the whole grid and every voxel is written.
+// non-void voxels may hold anything) the mask covers the whole grid and the non-void voxels of both
+// buffers are set to 0 first (every step keeps them 0).
 int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
                  cudaStream_t st, const int* zlimit, int full_first, uint8_t* mask, int* err) {
     int steps;
@@ -653,11 +708,16 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     c.vz_over_dz = p->vz > 0.0f ? p->vz / p->dz : 0.0f;
     c.dtp = dtp;
     c.decay = decay;
+    const PlumeTab tab = make_plume_tab(c);
     const int nx = p->nx, ny = p->ny, nz = p->nz;
     const int mz = plume_mask_pitch(nz);
     const int* zl = full_first ? nullptr : zlimit;
     k_plume_mask<<<dim3((ny + PM_TY - 1) / PM_TY, nx), dim3(PM_TZ, PM_TY), 0, st>>>(nx, ny, nz, mz, F, mask, zl);
     BD_CHECK_LAUNCH("k_plume_mask");
+    if (full_first) {
+        k_plume_clear<<<grid_for((int64_t)nx * ny * nz, 256), 256, 0, st>>>(Ca, Cb, mask, nx, ny, nz, mz);
+        BD_CHECK_LAUNCH("k_plume_clear");
+    }
     const long long total = (long long)steps * n_substeps;
     const int kernel = tune_value(BD_TUNE_PLUME_KERNEL);
     if (kernel == BD_PLUME_KERNEL_RESIDENT && total <= (1LL << 30)) {
@@ -668,7 +728,7 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
             a.M = mask; a.zlimit = zl; a.flags = resident_flags(mask, nx, ny, nz); a.err = err;
             a.nx = nx; a.ny = ny; a.nz = nz; a.mz = mz;
             a.tiles_x = plan.tiles_x; a.tiles_y = plan.tiles_y; a.n_steps = (int)total;
-            a.c = c;
+            a.k = tab;
             BD_CUDA(cudaMemsetAsync(a.flags, 0, sizeof(unsigned) * plan.grid, st));
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(plan.grid);
@@ -690,7 +750,7 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     const dim3 dgrid((nz + PL_BZ - 1) / PL_BZ, (ny + PD_BY - 1) / PD_BY, (nx + xc - 1) / xc);
     // live z groups per direct-kernel column, from this stage's mask
     uint8_t* zlist = nullptr;
-    if (vec && !full_first && (nz + 3) / 4 <= 255) {
+    if (vec && (nz + 3) / 4 <= 255) {
         zlist = mask + plume_zlist_offset(nx, ny, nz);
         k_plume_zlist<<<dim3((ny + PD_BY - 1) / PD_BY, (nx + xc - 1) / xc), 256, 0, st>>>(mask, nx, ny, nz, mz, xc, zl,
                                                                                           zlist);
@@ -699,15 +759,13 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     for (long long s = 0; s < total; ++s) {
         const float* in = (s & 1) ? Cb : Ca;
         float* out = (s & 1) ? Ca : Cb;
-        // the context API writes every voxel in the first two steps (one per ping-pong buffer)
-        const int full = (full_first && s < 2) ? 1 : 0;
         if (zlist)
-            k_plume_direct_z<<<dgrid, 8 * PD_BY, 0, st>>>(in, out, mask, nx, ny, nz, mz, xc, c, zl, zlist);
+            k_plume_direct_z<<<dgrid, 8 * PD_BY, 0, st>>>(in, out, mask, nx, ny, nz, mz, xc, tab, zl, zlist);
         else if (vec)
-            k_plume_direct<<<dgrid, 8 * PD_BY, 0, st>>>(in, out, mask, nx, ny, nz, mz, xc, c, zl, full);
+            k_plume_direct<<<dgrid, 8 * PD_BY, 0, st>>>(in, out, mask, nx, ny, nz, mz, xc, tab, zl);
         else
-            k_plume_step<<<dim3((ny + PM_TY - 1) / PM_TY, nx), dim3(PM_TZ, PM_TY), 0, st>>>(nx, ny, nz, mz, c, in, out,
-                                                                                        mask, zl, full);
+            k_plume_step<<<dim3((ny + PM_TY - 1) / PM_TY, nx), dim3(PM_TZ, PM_TY), 0, st>>>(nx, ny, nz, mz, tab, in, out,
+                                                                                        mask, zl);
     }
     BD_CHECK_LAUNCH("k_plume_step");
     if (in_b) *in_b = (int)(total & 1);
