@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-denoiser", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-full-run", action="store_true", help="skip the device-timed 1000-epoch schedule")
+    ap.add_argument("--plume-kernel", type=int, default=None, choices=[4, 5],
+                    help="plume kernel to use (4 direct, 5 resident) instead of the autotuner's choice")
     ap.add_argument("--workload", default="coupled", choices=["coupled", "campaign"],
                     help="coupled: the headline run; campaign: 24 wavelength x power x pulse instances at once")
     return ap.parse_args()
@@ -217,8 +219,13 @@ def run_ours(args, rank, world, local):
             e = make_engine(geo, dev, seed_offset=1000 + rank)
             e.laser_power = POWER_W
             return e
-        tuned = campaign.autotune(probe)
+        cand = None
+        if args.plume_kernel is not None:
+            cand = {_lib.TUNE_PLUME_KERNEL: [args.plume_kernel]}
+        tuned = campaign.autotune(probe, candidates=cand)
         torch.cuda.synchronize()
+    if args.plume_kernel is not None:
+        _lib.call("bd_tune_set", _lib.TUNE_PLUME_KERNEL, args.plume_kernel)
     from bug_defense_b200.replicas import replica_seed
     eng = make_engine(geo, dev, seed_offset=replica_seed(0, rank))
     K, W = int(args.steps), int(args.warmup)
