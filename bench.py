@@ -464,7 +464,7 @@ def denoised_run_leg(n_laser=10, check_every=5):
             torch.cuda.synchronize()
             row[f"{mode}_ms_per_laser_epoch"] = round(e0.elapsed_time(e1) / n_laser, 3)
             if run:
-                row["spot_check_rel_l2"] = [round(r, 4) for _, r in run.checks]
+                row["spot_checks"] = [{"rel_l2": round(r, 4), "bound": round(b, 4)} for _, r, b in run.checks]
                 row["fell_back"] = run.fallen_back
             del eng, run
         row["speedup"] = round(row["plain_ms_per_laser_epoch"] / row["denoised_ms_per_laser_epoch"], 3)

@@ -7,15 +7,17 @@ properties (plume extinction included), passes the noisy map, the optics and the
 through the trained network (denoise.Denoiser) and hands the denoised map to the engine as the
 epoch's absorbed map, in place of its own MC (the engine's fixed-map path: the epoch's substeps,
 phase update and plume run unchanged). Every `check_every` laser epochs the plain n_photons map is
-traced as well and the two are compared by relative L2; above `threshold` the run falls back to
-plain MC for good (that epoch already uses the plain map). Plain MC stays the judge of the
-network's error: the spot checks are returned with the diagnostics.
+traced as well, as two independent halves, and the two maps are compared by relative L2. With
+independent errors E||den - plain||^2 = err_den^2 + err_plain^2, and the halves give
+err_plain ~ sigma = ||h1 - h2|| / ||h1 + h2||, so the denoised map is at least as accurate as plain
+MC while ||den - plain|| / ||plain|| <= sqrt(2) sigma: above that bound (or above a fixed
+`threshold`, when one is given) the run falls back to plain MC for good (that epoch already uses the
+plain map). Plain MC stays the judge of the network's error: the spot checks are returned with the
+diagnostics.
 """
 from __future__ import annotations
 
-import ctypes
-
-import numpy as np
+import math
 
 from . import _lib
 
@@ -25,24 +27,26 @@ class DenoisedCoupledRun:
 
     engine: the engine (its n_photons is the plain photon count of the spot checks and fallback);
     denoiser: a denoise.Denoiser (default: the trained weights); lo_photons: photons per denoised
-    epoch; check_every: laser epochs between spot checks (0: never); threshold: relative L2 between
-    the denoised and the plain map above which the run falls back to plain MC."""
+    epoch; check_every: laser epochs between spot checks (0: never); threshold: a fixed relative L2
+    between the denoised and the plain map above which the run falls back to plain MC (None: the
+    equal-error bound sqrt(2) sigma of the plain map's own noise)."""
 
     def __init__(self, engine, denoiser=None, lo_photons: int = 15_000, check_every: int = 20,
-                 threshold: float = 0.35):
+                 threshold: float | None = None):
         import torch
         from . import denoise
         self.eng = engine
         self.den = denoiser if denoiser is not None else denoise.Denoiser.load()
         self.lo_photons = int(lo_photons)
         self.check_every = int(check_every)
-        self.threshold = float(threshold)
+        self.threshold = None if threshold is None else float(threshold)
         self.fallen_back = False
-        self.checks = []              # (epoch, relative L2 denoised vs plain)
+        self.checks = []              # (epoch, relative L2 denoised vs plain, the bound it was held to)
         self.laser_epochs = 0
         dev = engine.dev
         self._A_lo = torch.zeros(engine.shape, dtype=torch.float32, device=dev)
         self._A_pl = torch.zeros(engine.shape, dtype=torch.float32, device=dev)
+        self._A_pl2 = torch.zeros(engine.shape, dtype=torch.float32, device=dev)
         self._out = torch.empty(engine.shape, dtype=torch.float32, device=dev)
         self._ledger = torch.zeros(_lib.LEDGER_LEN, dtype=torch.float64, device=dev)
         self._enqueued = int(engine.epoch)
@@ -74,12 +78,18 @@ class DenoisedCoupledRun:
         den = self.den(self._A_lo, eng._props, eng._flags, out=self._out)
         use = den
         if self.check_every > 0 and self.laser_epochs % self.check_every == 0:
-            self._trace(eng.n_photons, self._A_pl, base + (1 << 30))
-            self._A_pl.mul_(1.0 / eng.n_photons)
-            rel = float(((den.double() - self._A_pl.double()).norm() / self._A_pl.double().norm()).item())
-            self.checks.append((e, rel))
-            if rel > self.threshold:
+            half = max(eng.n_photons // 2, 1)
+            self._trace(half, self._A_pl, base + (1 << 30))
+            self._trace(half, self._A_pl2, base + (1 << 30) + half)
+            h1, h2 = self._A_pl.double(), self._A_pl2.double()
+            plain = (h1 + h2) * (0.5 / half)
+            sigma = float(((h1 - h2).norm() / (h1 + h2).norm()).item())
+            rel = float(((den.double() - plain).norm() / plain.norm()).item())
+            bound = self.threshold if self.threshold is not None else math.sqrt(2.0) * sigma
+            self.checks.append((e, rel, bound))
+            if rel > bound:
                 self.fallen_back = True
+                self._A_pl.copy_(plain)
                 use = self._A_pl
         # the engine's tally holds absorbed weight for its n_photons launched photons
         eng._A.copy_(use)
