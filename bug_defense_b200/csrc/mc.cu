@@ -9,8 +9,9 @@
 //      face crossings do Fresnel/TIR or Snell at index steps, exits tally R_diff / T / lateral.
 //
 // B200 design:
-//   * one persistent grid, photons handed out by a global atomic queue so warps stay full
-//     while the per-photon step counts differ by orders of magnitude;
+//   * one persistent grid, photons handed out by a global atomic queue; every lane advances its
+//     photon by one event per loop iteration and takes a new photon as soon as its own ends, so
+//     warps stay full while the per-photon event counts differ by orders of magnitude;
 //   * Philox-4x32-10 counter-based RNG keyed on (seed, photon index): no RNG state in memory
 //     and a photon's path does not depend on which thread traced it;
 //   * optical properties packed as one float4 {mu_t, mu_a/mu_t, g, n} per voxel read through
@@ -152,209 +153,217 @@ struct ThreadLedger {
     unsigned collisions, crossings, reflections;
 };
 
-template <int DEPTH>  // 2: launch along +z at z=0 ; 0: launch along +x at x=0
-__device__ __forceinline__ void trace_photon(const McDev& P, long long pid, const float4* __restrict__ props,
-                                             const uint8_t* __restrict__ flags, float* __restrict__ A,
-                                             unsigned long long* __restrict__ A64, float* __restrict__ L,
-                                             double* __restrict__ latz, double* sl, ThreadLedger& tl) {
+// The photon a lane is tracing. The kernel advances every lane by one event per loop iteration,
+// and a lane whose photon has ended takes the next photon from the queue in the same loop, so the
+// lanes of a warp are not held back until the warp's longest photon ends (event counts per photon
+// differ by orders of magnitude). A photon's random stream and arithmetic do not depend on the
+// lane that traces it or on when it is traced.
+struct PhotonState {
     PhotonRng rng;
-    rng.init(P.seed, (unsigned long long)(P.offset + pid));
-    const bool metal = (P.options & BD_MC_METAL_SEMANTICS) != 0;
-    const bool tally_l = (P.options & BD_MC_TALLY_FLUENCE) != 0 && L != nullptr;
+    float x, y, z, ux, uy, uz, iux, iuy, iuz, tau, w;
+    float4 pr;
+    int ix, iy, iz, idx;
+    long long ev;
+};
 
+// Launch: transverse offsets, footprint test, entrance Fresnel split and refraction, first
+// optical depth. Returns false when the photon never enters the grid (booked here).
+template <int DEPTH>  // 2: launch along +z at z=0 ; 0: launch along +x at x=0
+__device__ __forceinline__ bool photon_launch(const McDev& P, long long pid, const float4* __restrict__ props,
+                                              double* __restrict__ latz, double* sl, PhotonState& s) {
+    s.rng.init(P.seed, (unsigned long long)(P.offset + pid));
     float u1, u2;
-    beam_offsets(P, rng, u1, u2);
-    float x, y, z;
-    int ix, iy, iz;
+    beam_offsets(P, s.rng, u1, u2);
     const float stretch = u1 / P.cos_th_safe;
     if (DEPTH == 2) {
-        x = P.xc + stretch * P.cos_ph - u2 * P.sin_ph;
-        y = P.yc + stretch * P.sin_ph + u2 * P.cos_ph;
-        z = 0.0f;
-        bool out = x < 0.0f || x >= P.lx || y < 0.0f || y >= P.ly;
+        s.x = P.xc + stretch * P.cos_ph - u2 * P.sin_ph;
+        s.y = P.yc + stretch * P.sin_ph + u2 * P.cos_ph;
+        s.z = 0.0f;
+        bool out = s.x < 0.0f || s.x >= P.lx || s.y < 0.0f || s.y >= P.ly;
         if (!out && P.rmax2 > 0.0f) {
-            float a = x - P.xc, b = y - P.yc;
+            float a = s.x - P.xc, b = s.y - P.yc;
             out = a * a + b * b >= P.rmax2;
         }
         if (out) {
             atomicAdd(&sl[BD_LEDGER_LATERAL], 1.0);
             if (latz) atomicAdd(&latz[0], 1.0);
-            return;
+            return false;
         }
-        ix = min((int)(x / P.dx), P.nx - 1);
-        iy = min((int)(y / P.dy), P.ny - 1);
-        iz = 0;
+        s.ix = min((int)(s.x / P.dx), P.nx - 1);
+        s.iy = min((int)(s.y / P.dy), P.ny - 1);
+        s.iz = 0;
     } else {
-        x = 0.0f;
-        y = P.yc + stretch * P.cos_ph - u2 * P.sin_ph;
-        z = P.zc + stretch * P.sin_ph + u2 * P.cos_ph;
-        bool out = y < 0.0f || y >= P.ly || z < 0.0f || z >= P.lz;
+        s.x = 0.0f;
+        s.y = P.yc + stretch * P.cos_ph - u2 * P.sin_ph;
+        s.z = P.zc + stretch * P.sin_ph + u2 * P.cos_ph;
+        bool out = s.y < 0.0f || s.y >= P.ly || s.z < 0.0f || s.z >= P.lz;
         if (!out && P.rmax2 > 0.0f) {
-            float a = y - P.yc, b = z - P.zc;
+            float a = s.y - P.yc, b = s.z - P.zc;
             out = a * a + b * b >= P.rmax2;
         }
         if (out) {
             atomicAdd(&sl[BD_LEDGER_LATERAL], 1.0);
             if (latz) atomicAdd(&latz[0], 1.0);
-            return;
+            return false;
         }
-        ix = 0;
-        iy = min((int)(y / P.dy), P.ny - 1);
-        iz = min((int)(z / P.dz), P.nz - 1);
+        s.ix = 0;
+        s.iy = min((int)(s.y / P.dy), P.ny - 1);
+        s.iz = min((int)(s.z / P.dz), P.nz - 1);
     }
-    float ux = P.ux0, uy = P.uy0, uz = P.uz0;
-    const int ny = P.ny, nz = P.nz;
-    const int sx_stride = ny * nz;
-    int idx = ix * sx_stride + iy * nz + iz;
+    s.ux = P.ux0; s.uy = P.uy0; s.uz = P.uz0;
+    s.idx = s.ix * (P.ny * P.nz) + s.iy * P.nz + s.iz;
 
     // entrance face: deterministic specular split + refraction (voxel_mc_3d.py:183-192)
-    float4 pr = __ldg(&props[idx]);
-    float w;
+    s.pr = __ldg(&props[s.idx]);
     {
-        float n_in = pr.w;
-        float cos_in = (DEPTH == 2) ? uz : ux;
+        float n_in = s.pr.w;
+        float cos_in = (DEPTH == 2) ? s.uz : s.ux;
         float r = fresnel_unpol(P.n_amb, n_in, cos_in, P.eq_eps);
-        w = 1.0f - r;
+        s.w = 1.0f - r;
         // the ledger books what the FP32 weight actually lost, so it closes exactly
-        atomicAdd(&sl[BD_LEDGER_SPECULAR], 1.0 - (double)w);
-        if (w <= 0.0f) return;
-        if (fabsf(n_in - P.n_amb) > P.entry_eps) refract_axis(ux, uy, uz, DEPTH, P.n_amb / n_in);
+        atomicAdd(&sl[BD_LEDGER_SPECULAR], 1.0 - (double)s.w);
+        if (s.w <= 0.0f) return false;
+        if (fabsf(n_in - P.n_amb) > P.entry_eps) refract_axis(s.ux, s.uy, s.uz, DEPTH, P.n_amb / n_in);
     }
-    float iux = fabsf(ux) > 1e-15f ? 1.0f / ux : 0.0f;
-    float iuy = fabsf(uy) > 1e-15f ? 1.0f / uy : 0.0f;
-    float iuz = fabsf(uz) > 1e-15f ? 1.0f / uz : 0.0f;
-    float tau = -__logf(fmaxf(rng.uniform(), 1e-12f));
+    s.iux = fabsf(s.ux) > 1e-15f ? 1.0f / s.ux : 0.0f;
+    s.iuy = fabsf(s.uy) > 1e-15f ? 1.0f / s.uy : 0.0f;
+    s.iuz = fabsf(s.uz) > 1e-15f ? 1.0f / s.uz : 0.0f;
+    s.tau = -__logf(fmaxf(s.rng.uniform(), 1e-12f));
+    s.ev = 0;
+    return true;
+}
 
+// One event of the hop-drop-spin loop (voxel_mc_3d.py:194-337): a collision inside the voxel or a
+// crossing of its exit face. Returns false when the photon has ended (its weight booked).
+template <int DEPTH>
+__device__ __forceinline__ bool photon_event(const McDev& P, const float4* __restrict__ props,
+                                             const uint8_t* __restrict__ flags, float* __restrict__ A,
+                                             unsigned long long* __restrict__ A64, float* __restrict__ L,
+                                             double* __restrict__ latz, double* sl, ThreadLedger& tl,
+                                             PhotonState& s, bool metal, bool tally_l) {
     const float dx = P.dx, dy = P.dy, dz = P.dz;
-    unsigned ncol = 0, ncross = 0, nrefl = 0;
-    for (int ev = 0; ev < P.max_events; ++ev) {
-        // exact ray/box distance to the exit face (voxel_mc_3d.py:72-98)
-        float sx = ux > 1e-15f ? ((float)(ix + 1) * dx - x) * iux : (ux < -1e-15f ? ((float)ix * dx - x) * iux : 1e30f);
-        float sy = uy > 1e-15f ? ((float)(iy + 1) * dy - y) * iuy : (uy < -1e-15f ? ((float)iy * dy - y) * iuy : 1e30f);
-        float sz = uz > 1e-15f ? ((float)(iz + 1) * dz - z) * iuz : (uz < -1e-15f ? ((float)iz * dz - z) * iuz : 1e30f);
-        int axis;
-        float s_exit;
-        if (sx <= sy && sx <= sz) { axis = 0; s_exit = fmaxf(sx, 0.0f); }
-        else if (sy <= sz)        { axis = 1; s_exit = fmaxf(sy, 0.0f); }
-        else                      { axis = 2; s_exit = fmaxf(sz, 0.0f); }
-        const float mu_t = pr.x;
+    // exact ray/box distance to the exit face (voxel_mc_3d.py:72-98)
+    float sx = s.ux > 1e-15f ? ((float)(s.ix + 1) * dx - s.x) * s.iux
+                             : (s.ux < -1e-15f ? ((float)s.ix * dx - s.x) * s.iux : 1e30f);
+    float sy = s.uy > 1e-15f ? ((float)(s.iy + 1) * dy - s.y) * s.iuy
+                             : (s.uy < -1e-15f ? ((float)s.iy * dy - s.y) * s.iuy : 1e30f);
+    float sz = s.uz > 1e-15f ? ((float)(s.iz + 1) * dz - s.z) * s.iuz
+                             : (s.uz < -1e-15f ? ((float)s.iz * dz - s.z) * s.iuz : 1e30f);
+    int axis;
+    float s_exit;
+    if (sx <= sy && sx <= sz) { axis = 0; s_exit = fmaxf(sx, 0.0f); }
+    else if (sy <= sz)        { axis = 1; s_exit = fmaxf(sy, 0.0f); }
+    else                      { axis = 2; s_exit = fmaxf(sz, 0.0f); }
+    const float mu_t = s.pr.x;
 
-        if (mu_t > 1e-12f && mu_t * s_exit >= tau) {
-            // ---- interaction inside the voxel ----
-            ++ncol;
-            float s = tau / mu_t;
-            if (tally_l) atomicAdd(&L[idx], w * s);
-            x += s * ux; y += s * uy; z += s * uz;
-            if (P.rmax2 > 0.0f) {
-                float a = (DEPTH == 2) ? x - P.xc : y - P.yc;
-                float b = (DEPTH == 2) ? y - P.yc : z - P.zc;
-                if (a * a + b * b >= P.rmax2) {
-                    atomicAdd(&sl[BD_LEDGER_LATERAL], (double)w);
-                    if (latz) atomicAdd(&latz[DEPTH == 2 ? iz : ix], (double)w);
-                    goto done;
-                }
-            }
-            {
-                const float dw = w * pr.y;
-                const float w_new = w - dw;
-                if (A64) atomicAdd(&A64[idx], __float2ull_rn(dw * kTallyScale));
-                else atomicAdd(&A[idx], dw);
-                const double lost = (double)w - (double)w_new;  // exact: both are FP32 values
-                if (flags != nullptr && (__ldg(&flags[idx]) & BD_FLAG_ABLATED)) atomicAdd(&sl[BD_LEDGER_ABSORBED_VOID], lost);
-                else tl.absorbed += lost;
-                w = w_new;
-            }
-            if (w < 1e-4f) {
-                if (rng.uniform() < 0.1f) {
-                    const float w10 = w * 10.0f;
-                    atomicAdd(&sl[BD_LEDGER_ROULETTE_GAIN], (double)w10 - (double)w);
-                    w = w10;
-                } else {
-                    atomicAdd(&sl[BD_LEDGER_ROULETTE_LOSS], (double)w);
-                    goto done;
-                }
-            }
-            scatter_hg(ux, uy, uz, pr.z, rng);
-            iux = fabsf(ux) > 1e-15f ? 1.0f / ux : 0.0f;
-            iuy = fabsf(uy) > 1e-15f ? 1.0f / uy : 0.0f;
-            iuz = fabsf(uz) > 1e-15f ? 1.0f / uz : 0.0f;
-            tau = -__logf(fmaxf(rng.uniform(), 1e-12f));
-            continue;
-        }
-
-        // ---- traverse the chord and land exactly on the exit face ----
-        ++ncross;
-        tau -= mu_t * s_exit;
-        if (tally_l) atomicAdd(&L[idx], w * s_exit);
-        x += s_exit * ux; y += s_exit * uy; z += s_exit * uz;
-        int jx = ix, jy = iy, jz = iz;
-        if (axis == 0)      { int sd = ux > 0.0f ? 1 : -1; jx += sd; x = sd > 0 ? (float)(ix + 1) * dx : (float)ix * dx; }
-        else if (axis == 1) { int sd = uy > 0.0f ? 1 : -1; jy += sd; y = sd > 0 ? (float)(iy + 1) * dy : (float)iy * dy; }
-        else                { int sd = uz > 0.0f ? 1 : -1; jz += sd; z = sd > 0 ? (float)(iz + 1) * dz : (float)iz * dz; }
-
-        if (axis == DEPTH) {
-            const int jd = (DEPTH == 2) ? jz : jx;
-            const int nd = (DEPTH == 2) ? P.nz : P.nx;
-            if (jd < 0) {
-                // leaving through the entrance face: Fresnel / TIR against ambient
-                float cos_out = (DEPTH == 2) ? uz : ux;
-                float r = fresnel_unpol(pr.w, P.n_amb, cos_out, P.eq_eps);
-                if (r > 0.0f && rng.uniform() < r) {
-                    ++nrefl;
-                    if (DEPTH == 2) { uz = -uz; iuz = -iuz; } else { ux = -ux; iux = -iux; }
-                    continue;
-                }
-                atomicAdd(&sl[BD_LEDGER_DIFFUSE], (double)w);
-                goto done;
-            }
-            if (jd >= nd) {
-                atomicAdd(&sl[BD_LEDGER_TRANSMITTED], (double)w);
-                goto done;
-            }
-        } else if (jx < 0 || jx >= P.nx || jy < 0 || jy >= P.ny || jz < 0 || jz >= P.nz) {
-            atomicAdd(&sl[BD_LEDGER_LATERAL], (double)w);
-            if (latz) atomicAdd(&latz[DEPTH == 2 ? iz : ix], (double)w);
-            goto done;
-        }
-        if (!metal && P.rmax2 > 0.0f) {
-            float a = (DEPTH == 2) ? x - P.xc : y - P.yc;
-            float b = (DEPTH == 2) ? y - P.yc : z - P.zc;
+    if (mu_t > 1e-12f && mu_t * s_exit >= s.tau) {
+        // ---- interaction inside the voxel ----
+        ++tl.collisions;
+        float st = s.tau / mu_t;
+        if (tally_l) atomicAdd(&L[s.idx], s.w * st);
+        s.x += st * s.ux; s.y += st * s.uy; s.z += st * s.uz;
+        if (P.rmax2 > 0.0f) {
+            float a = (DEPTH == 2) ? s.x - P.xc : s.y - P.yc;
+            float b = (DEPTH == 2) ? s.y - P.yc : s.z - P.zc;
             if (a * a + b * b >= P.rmax2) {
-                atomicAdd(&sl[BD_LEDGER_LATERAL], (double)w);
-                if (latz) atomicAdd(&latz[DEPTH == 2 ? iz : ix], (double)w);
-                goto done;
+                atomicAdd(&sl[BD_LEDGER_LATERAL], (double)s.w);
+                if (latz) atomicAdd(&latz[DEPTH == 2 ? s.iz : s.ix], (double)s.w);
+                return false;
             }
         }
         {
-            const int jidx = jx * sx_stride + jy * nz + jz;
-            float4 pn = __ldg(&props[jidx]);
-            float n1 = pr.w, n2 = pn.w;
-            if (fabsf(n1 - n2) > P.step_eps) {
-                float cos_face = axis == 0 ? ux : (axis == 1 ? uy : uz);
-                float r = fresnel_unpol(n1, n2, cos_face, P.eq_eps);
-                if ((!metal || r > 0.0f) && rng.uniform() < r) {
-                    ++nrefl;
-                    if (axis == 0) { ux = -ux; iux = -iux; }
-                    else if (axis == 1) { uy = -uy; iuy = -iuy; }
-                    else { uz = -uz; iuz = -iuz; }
-                    continue;
-                }
-                refract_axis(ux, uy, uz, axis, n1 / n2);
-                iux = fabsf(ux) > 1e-15f ? 1.0f / ux : 0.0f;
-                iuy = fabsf(uy) > 1e-15f ? 1.0f / uy : 0.0f;
-                iuz = fabsf(uz) > 1e-15f ? 1.0f / uz : 0.0f;
+            const float dw = s.w * s.pr.y;
+            const float w_new = s.w - dw;
+            if (A64) atomicAdd(&A64[s.idx], __float2ull_rn(dw * kTallyScale));
+            else atomicAdd(&A[s.idx], dw);
+            const double lost = (double)s.w - (double)w_new;  // exact: both are FP32 values
+            if (flags != nullptr && (__ldg(&flags[s.idx]) & BD_FLAG_ABLATED)) atomicAdd(&sl[BD_LEDGER_ABSORBED_VOID], lost);
+            else tl.absorbed += lost;
+            s.w = w_new;
+        }
+        if (s.w < 1e-4f) {
+            if (s.rng.uniform() < 0.1f) {
+                const float w10 = s.w * 10.0f;
+                atomicAdd(&sl[BD_LEDGER_ROULETTE_GAIN], (double)w10 - (double)s.w);
+                s.w = w10;
+            } else {
+                atomicAdd(&sl[BD_LEDGER_ROULETTE_LOSS], (double)s.w);
+                return false;
             }
-            ix = jx; iy = jy; iz = jz;
-            idx = jidx;
-            pr = pn;
+        }
+        scatter_hg(s.ux, s.uy, s.uz, s.pr.z, s.rng);
+        s.iux = fabsf(s.ux) > 1e-15f ? 1.0f / s.ux : 0.0f;
+        s.iuy = fabsf(s.uy) > 1e-15f ? 1.0f / s.uy : 0.0f;
+        s.iuz = fabsf(s.uz) > 1e-15f ? 1.0f / s.uz : 0.0f;
+        s.tau = -__logf(fmaxf(s.rng.uniform(), 1e-12f));
+        return true;
+    }
+
+    // ---- traverse the chord and land exactly on the exit face ----
+    ++tl.crossings;
+    s.tau -= mu_t * s_exit;
+    if (tally_l) atomicAdd(&L[s.idx], s.w * s_exit);
+    s.x += s_exit * s.ux; s.y += s_exit * s.uy; s.z += s_exit * s.uz;
+    int jx = s.ix, jy = s.iy, jz = s.iz;
+    if (axis == 0)      { int sd = s.ux > 0.0f ? 1 : -1; jx += sd; s.x = sd > 0 ? (float)(s.ix + 1) * dx : (float)s.ix * dx; }
+    else if (axis == 1) { int sd = s.uy > 0.0f ? 1 : -1; jy += sd; s.y = sd > 0 ? (float)(s.iy + 1) * dy : (float)s.iy * dy; }
+    else                { int sd = s.uz > 0.0f ? 1 : -1; jz += sd; s.z = sd > 0 ? (float)(s.iz + 1) * dz : (float)s.iz * dz; }
+
+    if (axis == DEPTH) {
+        const int jd = (DEPTH == 2) ? jz : jx;
+        const int nd = (DEPTH == 2) ? P.nz : P.nx;
+        if (jd < 0) {
+            // leaving through the entrance face: Fresnel / TIR against ambient
+            float cos_out = (DEPTH == 2) ? s.uz : s.ux;
+            float r = fresnel_unpol(s.pr.w, P.n_amb, cos_out, P.eq_eps);
+            if (r > 0.0f && s.rng.uniform() < r) {
+                ++tl.reflections;
+                if (DEPTH == 2) { s.uz = -s.uz; s.iuz = -s.iuz; } else { s.ux = -s.ux; s.iux = -s.iux; }
+                return true;
+            }
+            atomicAdd(&sl[BD_LEDGER_DIFFUSE], (double)s.w);
+            return false;
+        }
+        if (jd >= nd) {
+            atomicAdd(&sl[BD_LEDGER_TRANSMITTED], (double)s.w);
+            return false;
+        }
+    } else if (jx < 0 || jx >= P.nx || jy < 0 || jy >= P.ny || jz < 0 || jz >= P.nz) {
+        atomicAdd(&sl[BD_LEDGER_LATERAL], (double)s.w);
+        if (latz) atomicAdd(&latz[DEPTH == 2 ? s.iz : s.ix], (double)s.w);
+        return false;
+    }
+    if (!metal && P.rmax2 > 0.0f) {
+        float a = (DEPTH == 2) ? s.x - P.xc : s.y - P.yc;
+        float b = (DEPTH == 2) ? s.y - P.yc : s.z - P.zc;
+        if (a * a + b * b >= P.rmax2) {
+            atomicAdd(&sl[BD_LEDGER_LATERAL], (double)s.w);
+            if (latz) atomicAdd(&latz[DEPTH == 2 ? s.iz : s.ix], (double)s.w);
+            return false;
         }
     }
-    // event cap reached: the remaining weight is accounted, not lost
-    atomicAdd(&sl[BD_LEDGER_TRUNCATED], (double)w);
-done:
-    tl.collisions += ncol;
-    tl.crossings += ncross;
-    tl.reflections += nrefl;
+    const int jidx = jx * (P.ny * P.nz) + jy * P.nz + jz;
+    float4 pn = __ldg(&props[jidx]);
+    float n1 = s.pr.w, n2 = pn.w;
+    if (fabsf(n1 - n2) > P.step_eps) {
+        float cos_face = axis == 0 ? s.ux : (axis == 1 ? s.uy : s.uz);
+        float r = fresnel_unpol(n1, n2, cos_face, P.eq_eps);
+        if ((!metal || r > 0.0f) && s.rng.uniform() < r) {
+            ++tl.reflections;
+            if (axis == 0) { s.ux = -s.ux; s.iux = -s.iux; }
+            else if (axis == 1) { s.uy = -s.uy; s.iuy = -s.iuy; }
+            else { s.uz = -s.uz; s.iuz = -s.iuz; }
+            return true;
+        }
+        refract_axis(s.ux, s.uy, s.uz, axis, n1 / n2);
+        s.iux = fabsf(s.ux) > 1e-15f ? 1.0f / s.ux : 0.0f;
+        s.iuy = fabsf(s.uy) > 1e-15f ? 1.0f / s.uy : 0.0f;
+        s.iuz = fabsf(s.uz) > 1e-15f ? 1.0f / s.uz : 0.0f;
+    }
+    s.ix = jx; s.iy = jy; s.iz = jz;
+    s.idx = jidx;
+    s.pr = pn;
+    return true;
 }
 
 #ifndef BD_MC_MIN_BLOCKS
@@ -374,12 +383,27 @@ __global__ void __launch_bounds__(128, BD_MC_MIN_BLOCKS) k_mc_trace(McDev P, con
     ThreadLedger tl;
     tl.absorbed = 0.0;
     tl.collisions = tl.crossings = tl.reflections = 0u;
+    const bool metal = (P.options & BD_MC_METAL_SEMANTICS) != 0;
+    const bool tally_l = (P.options & BD_MC_TALLY_FLUENCE) != 0 && L != nullptr;
 
     const unsigned long long N = (unsigned long long)P.n_photons;
+    PhotonState s;
+    bool live = false;
     for (;;) {
-        unsigned long long p = atomicAdd(queue, 1ull);
-        if (p >= N) break;
-        trace_photon<DEPTH>(P, (long long)p, props, flags, A, A64, L, latz, sl, tl);
+        if (!live) {
+            const unsigned long long p = atomicAdd(queue, 1ull);
+            if (p >= N) break;
+            live = photon_launch<DEPTH>(P, (long long)p, props, latz, sl, s);
+            if (!live) continue;
+        }
+        if (s.ev >= P.max_events) {
+            // event cap reached: the remaining weight is accounted, not lost
+            atomicAdd(&sl[BD_LEDGER_TRUNCATED], (double)s.w);
+            live = false;
+            continue;
+        }
+        ++s.ev;
+        live = photon_event<DEPTH>(P, props, flags, A, A64, L, latz, sl, tl, s, metal, tally_l);
     }
     // warp reduction of the per-thread channels, one FP64 atomic per warp and channel
     double v0 = tl.absorbed;
