@@ -49,8 +49,9 @@ def parse():
     ap.add_argument("--no-denoiser", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-full-run", action="store_true", help="skip the device-timed 1000-epoch schedule")
-    ap.add_argument("--plume-kernel", type=int, default=None, choices=[4, 5],
-                    help="plume kernel to use (4 direct, 5 resident) instead of the autotuner's choice")
+    ap.add_argument("--plume-kernel", type=int, default=None, choices=[4, 5, 6],
+                    help="plume kernel to use (4 direct, 5 resident, 6 direct over a compact unit list) instead of "
+                         "the autotuner's choice")
     ap.add_argument("--workload", default="coupled", choices=["coupled", "campaign"],
                     help="coupled: the headline run; campaign: 24 wavelength x power x pulse instances at once")
     return ap.parse_args()
@@ -67,6 +68,26 @@ def measured_peaks():
         d = json.loads(p.read_text())
         return float(d.get("hbm_gbs", FALLBACK_HBM_GBS)), "measured", d
     return FALLBACK_HBM_GBS, "fallback", {}
+
+
+def l2_copy_gbs(dev, mbytes: int = 16, reps: int = 200) -> float:
+    """Copy bandwidth of an L2-resident pair of buffers (2 x `mbytes` MB, well inside the 126 MB
+    L2): GB/s of bytes read + written, CUDA events around `reps` device-to-device copies after a
+    warm-up. The denominator of the plume step's L2 fraction (its field stays in L2 between steps)."""
+    import torch
+    n = mbytes * (1 << 20) // 4
+    a = torch.ones(n, dtype=torch.float32, device=dev)
+    b = torch.empty_like(a)
+    for _ in range(10):
+        b.copy_(a)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    for _ in range(reps):
+        b.copy_(a)
+    e1.record()
+    e1.synchronize()
+    return 2.0 * a.numel() * 4 * reps / (e0.elapsed_time(e1) * 1e-3) / 1e9
 
 
 class ClockSampler:
@@ -360,7 +381,8 @@ def ours_main(args):
     from bug_defense_b200 import _lib
     kv = ctypes.c_int(0)
     _lib.call("bd_tune_get", _lib.TUNE_PLUME_KERNEL, ctypes.byref(kv))
-    plume_kernel = {4: "k_plume_direct_z", 5: "k_plume_resident"}.get(kv.value, "k_plume_step")
+    plume_kernel = {4: "k_plume_direct_z", 5: "k_plume_resident",
+                    6: "k_plume_direct_z<compact units>"}.get(kv.value, "k_plume_step")
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
@@ -375,6 +397,11 @@ def ours_main(args):
             "avg_launch_ms": round(per_launch[dom], 5),
             "units_per_launch": ("voxel-substeps" if dom == "substeps" else "plume (void) voxel-steps"),
             "void_voxels": int(n_void)}
+    if dom == "plume":
+        l2 = l2_copy_gbs(eng.dev)
+        roof.update({"l2_peak": round(l2, 1), "l2_frac": round(achieved / l2, 4),
+                     "l2_method": "device-to-device copy of a 16 MB float32 buffer into another (L2-resident), "
+                                  "read + written bytes / event time over 200 copies, measured in this run"})
     led = r["last_diag"]["ledger"]
     mc_ms = stage[0]
     photons = r["n_on"] * eng.n_photons

@@ -175,30 +175,36 @@ def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=
     """Pick launch shapes by timing them on a throwaway engine of the real workload: `inst` is a
     campaign instance dict or a callable returning an engine with a `laser_power` attribute.
     MC CTAs per SM (photons per thread) are timed by the MC stage of laser-on epochs; x-planes per
-    CTA of the fused substep kernel, the plume kernel (resident or one launch per step) and the
-    direct plume kernel's x-planes per CTA by the whole epoch with the laser off, when the void
-    domain does not change between trials. Sets the winning values process-wide (bd_tune_set) and returns the
-    choices with every trial's time (ms per epoch)."""
+    CTA of the fused substep kernel by the whole epoch with the laser off (the void domain does not
+    change between trials). The plume kernel and the direct kernel's x-planes per CTA are searched
+    together, also by laser-off epochs; the resident kernel has no x-planes knob and the compact
+    kernel chooses its x-planes per stage on the device. Sets
+    the winning values process-wide (bd_tune_set) and returns the choices with every trial's time
+    (ms per epoch)."""
     from . import _lib
     cand = dict(candidates or {})
     cand.setdefault(_lib.TUNE_MC_BLOCKS_PER_SM, [2, 4, 6, 8])
     cand.setdefault(_lib.TUNE_STENCIL_XC, [4, 8, 16])
-    cand.setdefault(_lib.TUNE_PLUME_KERNEL, [_lib.PLUME_KERNEL_DIRECT, _lib.PLUME_KERNEL_RESIDENT])
+    cand.setdefault(_lib.TUNE_PLUME_KERNEL, [_lib.PLUME_KERNEL_DIRECT, _lib.PLUME_KERNEL_COMPACT,
+                                             _lib.PLUME_KERNEL_RESIDENT])
     cand.setdefault(_lib.TUNE_PLUME_XC, [2, 3, 4, 6])
-    stage = {_lib.TUNE_MC_BLOCKS_PER_SM: 0, _lib.TUNE_STENCIL_XC: 1, _lib.TUNE_PLUME_XC: 2, _lib.TUNE_PLUME_KERNEL: 2}
     names = {_lib.TUNE_MC_BLOCKS_PER_SM: "mc_ctas_per_sm", _lib.TUNE_STENCIL_XC: "stencil_xc",
              _lib.TUNE_PLUME_XC: "plume_xc", _lib.TUNE_PLUME_KERNEL: "plume_kernel"}
     eng = inst() if callable(inst) else make_engine(inst, device=device)
     eng.step_epochs(3)                       # warm-up: graphs, caches, a first crater
     out = {"trials": {}}
-    for knob, values in cand.items():
-        trials = []
-        mc = knob == _lib.TUNE_MC_BLOCKS_PER_SM
-        for v in values:
+
+    def trial(settings, mc=False):
+        for knob, v in settings:
             _lib.call("bd_tune_set", int(knob), int(v))
-            _stage_ms(eng, 1, laser=mc)      # re-capture the stage graphs for the new shape
-            t = (float(_stage_ms(eng, epochs_per_trial, laser=True)[stage[knob]]) if mc
-                 else _epoch_ms(eng, epochs_per_trial, laser=False))
+        _stage_ms(eng, 1, laser=mc)          # re-capture the stage graphs for the new shape
+        return (float(_stage_ms(eng, epochs_per_trial, laser=True)[0]) if mc
+                else _epoch_ms(eng, epochs_per_trial, laser=False))
+
+    for knob in (_lib.TUNE_MC_BLOCKS_PER_SM, _lib.TUNE_STENCIL_XC):
+        trials = []
+        for v in cand[knob]:
+            t = trial([(knob, v)], mc=knob == _lib.TUNE_MC_BLOCKS_PER_SM)
             trials.append((int(v), t))
             if log:
                 log(f"autotune {names[knob]}={v}: {t:.3f} ms/epoch")
@@ -206,6 +212,27 @@ def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=
         _lib.call("bd_tune_set", int(knob), int(best))
         out[names[knob]] = best
         out["trials"][names[knob]] = trials
+    # plume kernel x x-planes per CTA (only the one-launch-per-step grid kernel takes the knob)
+    trials = []
+    for kern in cand[_lib.TUNE_PLUME_KERNEL]:
+        xcs = cand[_lib.TUNE_PLUME_XC] if kern == _lib.PLUME_KERNEL_DIRECT else [None]
+        for xc in xcs:
+            sets = [(_lib.TUNE_PLUME_KERNEL, kern)] + ([] if xc is None else [(_lib.TUNE_PLUME_XC, xc)])
+            t = trial(sets)
+            trials.append((int(kern), xc, t))
+            if log:
+                log(f"autotune plume_kernel={kern} plume_xc={xc}: {t:.3f} ms/epoch")
+    kern, xc, _ = min(trials, key=lambda t: t[2])
+    _lib.call("bd_tune_set", _lib.TUNE_PLUME_KERNEL, kern)
+    if xc is not None:
+        _lib.call("bd_tune_set", _lib.TUNE_PLUME_XC, xc)
+    else:
+        xv = ctypes.c_int(0)
+        _lib.call("bd_tune_get", _lib.TUNE_PLUME_XC, ctypes.byref(xv))
+        xc = xv.value
+    out["plume_kernel"] = kern
+    out["plume_xc"] = int(xc)
+    out["trials"]["plume"] = [[k, x, t] for k, x, t in trials]
     del eng
     return out
 

@@ -36,10 +36,24 @@ inline size_t plume_zlist_bytes(int nx, int ny, int nz) {
     const size_t cols = (size_t)nx * ((ny + kPlumeZRows - 1) / kPlumeZRows);
     return (cols * (1 + (size_t)(nz + 3) / 4) + 255) / 256 * 256;
 }
+// Then the compact-order state of the direct plume kernel: 16 header words (unit count, chosen
+// x planes per unit, unit count per candidate), the live-group bitmaps of every (x plane, y tile)
+// (8 words each), then the units (column << 5 | band), at most one per band of every column.
+inline size_t plume_units_offset(int nx, int ny, int nz) {
+    return plume_zlist_offset(nx, ny, nz) + plume_zlist_bytes(nx, ny, nz);
+}
+inline size_t plume_units_bytes(int nx, int ny, int nz) {
+    const size_t cols = (size_t)nx * ((ny + kPlumeZRows - 1) / kPlumeZRows);
+    const size_t bands = ((size_t)(nz + 3) / 4 + 7) / 8;
+    return ((16 + cols * 8 + cols * bands) * sizeof(unsigned) + 255) / 256 * 256;
+}
 // Then the per-CTA step counters of the resident plume kernel (at most kPlumeMaxTiles CTAs).
 constexpr int kPlumeMaxTiles = 256;
+inline size_t plume_flags_offset(int nx, int ny, int nz) {
+    return plume_units_offset(nx, ny, nz) + plume_units_bytes(nx, ny, nz);
+}
 inline size_t plume_mask_bytes(int nx, int ny, int nz) {
-    return plume_zlist_offset(nx, ny, nz) + plume_zlist_bytes(nx, ny, nz) + sizeof(unsigned) * kPlumeMaxTiles;
+    return plume_flags_offset(nx, ny, nz) + sizeof(unsigned) * kPlumeMaxTiles;
 }
 
 // Launch-shape knobs (BD_TUNE_*) and the generation counter bumped by every change.

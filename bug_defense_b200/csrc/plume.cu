@@ -8,12 +8,15 @@
 //                     and swaps a one-voxel halo with its four neighbours through L2 per step
 //   k_plume_direct_z  default (BD_PLUME_KERNEL_DIRECT): one launch per step, a CTA per 32 (z) x 16 (y)
 //                     tile column marching x planes over the column's live z groups
+//   k_plume_direct_c  (BD_PLUME_KERNEL_COMPACT): the same per-unit code, one wave of CTAs looping
+//                     over a compact list of the live units, x planes per unit chosen per stage
 //   k_plume_step      any grid (nz % 4 != 0): one voxel per thread
 // Layout: C-order (nx, ny, nz), z fastest; the neighbourhood of every voxel is one mask byte.
 #include "common.cuh"
 #include "engine.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 
 namespace bd {
@@ -312,35 +315,27 @@ __global__ void __launch_bounds__(256) k_plume_zlist(const uint8_t* __restrict__
     }
 }
 
-// As k_plume_direct, but band blockIdx.x of a column takes the column's live groups 8 b .. 8 b + 7
-// from its z list instead of 8 consecutive groups, so z tiles that are partly tissue cost only
-// their void groups. A lane whose z neighbour group is not held by the neighbouring lane loads that
-// neighbour voxel instead of taking it by shuffle. Voxels outside the lists are not void and are
-// never written.
-__global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_z(const float* __restrict__ C, float* __restrict__ Cn,
-                                                                 const uint8_t* __restrict__ M, int nx, int ny,
-                                                                 int nz, int mz, int xc,
-                                                                 const __grid_constant__ PlumeTab k,
-                                                                 const int* __restrict__ zlimit,
-                                                                 const uint8_t* __restrict__ zlist) {
-    __shared__ float w0s[64];
-    if (threadIdx.x < 64) w0s[threadIdx.x] = k.w0eff[threadIdx.x];
-    __syncthreads();
-    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
+// One unit of the direct kernel: band `band` of column `col` (y tile yt, x chunk xch of xc planes)
+// takes the column's live groups 8 band .. 8 band + 7 from its z list instead of 8 consecutive
+// groups, so z tiles that are partly tissue cost only their void groups. A lane whose z neighbour
+// group is not held by the neighbouring lane loads that neighbour voxel instead of taking it by
+// shuffle. Voxels outside the lists are not void and are never written. Uniform over the CTA.
+__device__ __forceinline__ void plume_direct_unit(const float* __restrict__ C, float* __restrict__ Cn,
+                                                  const uint8_t* __restrict__ M, int nx, int ny, int nz, int mz,
+                                                  int xc, const PlumeTab& k, int zl, const uint8_t* __restrict__ zlist,
+                                                  int n_cols, int col, int yt, int xch, int band, const float* w0s) {
     const int G = (nz + 3) / 4;
-    const int n_cols = gridDim.y * gridDim.z;
-    const int col = blockIdx.z * gridDim.y + blockIdx.y;
     const int cnt = zlist[col];
-    const int b0 = blockIdx.x * 8;
-    const int ib = blockIdx.z * xc, ie = min(nx, ib + xc);
-    if (b0 >= cnt || ib >= ie) return;  // uniform over the CTA
+    const int b0 = band * 8;
+    const int ib = xch * xc, ie = min(nx, ib + xc);
+    if (b0 >= cnt || ib >= ie) return;
     const int zg = threadIdx.x & 7;
     const int g = b0 + zg < cnt ? (int)zlist[n_cols + (size_t)col * G + b0 + zg] : -2;
     const int gp = __shfl_up_sync(0xffffffffu, g, 1, 8);
     const int gn = __shfl_down_sync(0xffffffffu, g, 1, 8);
     const bool zb_lane = zg > 0 && gp == g - 1;  // the -z neighbour is the previous lane's last voxel
     const bool zt_lane = zg < 7 && gn == g + 1;  // the +z neighbour is the next lane's first voxel
-    const int j = blockIdx.y * PD_BY + (threadIdx.x >> 3), z = 4 * max(g, 0);
+    const int j = yt * PD_BY + (threadIdx.x >> 3), z = 4 * max(g, 0);
     const bool act = g >= 0 && zl - z > 0 && j < ny;
     const bool in = g >= 0 && j < ny && z < nz;
     const unsigned zkeep = zkeep_mask(zl, z);
@@ -370,6 +365,190 @@ __global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_z(const float* __
         }
         cw = cc;
         cc = ce;
+    }
+}
+
+// BD_PLUME_KERNEL_DIRECT: grid (bands, y tiles, x chunks); CTAs past a column's live bands exit at once.
+__global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_z(const float* __restrict__ C, float* __restrict__ Cn,
+                                                                 const uint8_t* __restrict__ M, int nx, int ny,
+                                                                 int nz, int mz, int xc,
+                                                                 const __grid_constant__ PlumeTab k,
+                                                                 const int* __restrict__ zlimit,
+                                                                 const uint8_t* __restrict__ zlist) {
+    __shared__ float w0s[64];
+    if (threadIdx.x < 64) w0s[threadIdx.x] = k.w0eff[threadIdx.x];
+    __syncthreads();
+    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
+    const int col = blockIdx.z * gridDim.y + blockIdx.y;
+    plume_direct_unit(C, Cn, M, nx, ny, nz, mz, xc, k, zl, zlist, gridDim.y * gridDim.z, col, blockIdx.y, blockIdx.z,
+                      blockIdx.x, w0s);
+}
+
+// ---- BD_PLUME_KERNEL_COMPACT: the direct kernel over a compact list of live units ------------
+// A step's CTAs are dispatched at a limited rate and the step ends with its last CTA, so the step is
+// fastest when the live units about fill one wave of resident CTAs: each CTA then runs exactly one
+// unit, and no empty CTA is dispatched between working ones. Once per stage the x planes per unit
+// (xc) are chosen on the device: per (x plane, y tile) bitmaps of the live z groups give the unit
+// count of every candidate xc, and the smallest xc whose count fits the wave (3 % over allowed)
+// wins (fewer planes per unit = a shorter CTA). The z list and the unit list are then built for it
+// and the step kernel, one wave of CTAs, loops over the units. Region layout (32-bit words, from
+// plume_units_offset): [0] unit count, [1] chosen xc, [4 + c - kPlumeXcMin] unit count for xc = c,
+// then the bitmaps (nx x y tiles x kPlumeBitWords), then the units (column << 5 | band).
+constexpr int kPlumeXcMin = 2, kPlumeXcMax = 12;
+constexpr int kPlumeBitWords = 8;  // 32-group words of a bitmap: 4-voxel groups <= 255
+constexpr int kPlumeHdrWords = 16;
+
+// bit g of (x plane i, y tile yt): a voxel of group g below the void z-limit in the tile's rows is void
+__global__ void __launch_bounds__(256) k_plume_planebits(const uint8_t* __restrict__ M, int nx, int ny, int nz,
+                                                         int mz, const int* __restrict__ zlimit,
+                                                         unsigned* __restrict__ bits) {
+    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
+    const int G = (nz + 3) / 4;
+    const int yt = blockIdx.x, i = blockIdx.y, n_yt = gridDim.x;
+    const int j0 = yt * PD_BY, j1 = min(ny, j0 + PD_BY);
+    const int g = threadIdx.x;
+    bool live = false;
+    if (g < G && zl - 4 * g > 0) {
+        const unsigned keep = zkeep_mask(zl, 4 * g);
+        for (int j = j0; j < j1 && !live; ++j)
+            live = (__ldg(reinterpret_cast<const unsigned*>(M + ((size_t)i * ny + j) * mz + 4 * g)) & keep &
+                    0x40404040u) != 0u;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, live);
+    if ((threadIdx.x & 31) == 0) bits[((size_t)i * n_yt + yt) * kPlumeBitWords + (threadIdx.x >> 5)] = bal;
+}
+
+// live units (bands of 8 live groups) for candidate xc = kPlumeXcMin + blockIdx.x
+__global__ void __launch_bounds__(1024) k_plume_unit_counts(const unsigned* __restrict__ bits, int nx, int n_yt,
+                                                            int G, unsigned* __restrict__ hdr) {
+    __shared__ int tot;
+    if (threadIdx.x == 0) tot = 0;
+    __syncthreads();
+    const int c = kPlumeXcMin + blockIdx.x;
+    const int n_xch = (nx + c - 1) / c;
+    const int W = (G + 31) / 32;
+    int mine = 0;
+    for (int p = threadIdx.x; p < n_xch * n_yt; p += blockDim.x) {
+        const int xch = p / n_yt, yt = p - xch * n_yt;
+        const int ib = xch * c, ie = min(nx, ib + c);
+        int live = 0;
+        for (int w = 0; w < W; ++w) {
+            unsigned o = 0u;
+            for (int i = ib; i < ie; ++i) o |= __ldg(&bits[((size_t)i * n_yt + yt) * kPlumeBitWords + w]);
+            live += __popc(o);
+        }
+        mine += (live + 7) / 8;
+    }
+    atomicAdd(&tot, mine);
+    __syncthreads();
+    if (threadIdx.x == 0) hdr[4 + blockIdx.x] = (unsigned)tot;
+}
+
+// the smallest candidate xc whose unit count fits slot_cap (else the largest)
+__global__ void k_plume_pick_xc(unsigned* __restrict__ hdr, int slot_cap) {
+    if (threadIdx.x != 0) return;
+    int pick = kPlumeXcMax;
+    for (int c = kPlumeXcMin; c <= kPlumeXcMax; ++c)
+        if ((int)hdr[4 + c - kPlumeXcMin] <= slot_cap) {
+            pick = c;
+            break;
+        }
+    hdr[1] = (unsigned)pick;
+}
+
+// z lists of the chosen xc's columns from the bitmaps (the layout of k_plume_zlist's lists); grid
+// (y tiles, x chunks of the smallest candidate), chunks past the chosen xc's exit
+__global__ void __launch_bounds__(256) k_plume_zlist_bits(const unsigned* __restrict__ bits, int nx, int nz,
+                                                          const unsigned* __restrict__ hdr,
+                                                          uint8_t* __restrict__ zlist) {
+    __shared__ int wcount[8];
+    const int c = (int)hdr[1];
+    const int n_xch = (nx + c - 1) / c;
+    const int yt = blockIdx.x, xch = blockIdx.y, n_yt = gridDim.x;
+    if (xch >= n_xch) return;  // uniform over the CTA
+    const int G = (nz + 3) / 4;
+    const int n_cols = n_yt * n_xch;
+    const int col = xch * n_yt + yt;
+    const int ib = xch * c, ie = min(nx, ib + c);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned o = 0u;
+    if (32 * w < G)
+        for (int i = ib; i < ie; ++i) o |= __ldg(&bits[((size_t)i * n_yt + yt) * kPlumeBitWords + w]);
+    const int g = threadIdx.x;
+    const bool live = g < G && ((o >> lane) & 1u);
+    const unsigned bal = __ballot_sync(0xffffffffu, live);
+    if (lane == 0) wcount[w] = __popc(bal);
+    __syncthreads();
+    int before = 0;
+    for (int q = 0; q < w; ++q) before += wcount[q];
+    if (live) zlist[n_cols + (size_t)col * G + before + __popc(bal & ((1u << lane) - 1u))] = (uint8_t)g;
+    if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int q = 0; q < 8; ++q) tot += wcount[q];
+        zlist[col] = (uint8_t)tot;
+    }
+}
+
+// the unit list of the chosen xc's columns, in column order: one CTA, a block-wide exclusive scan
+// of the bands per column
+__global__ void __launch_bounds__(1024) k_plume_units(const uint8_t* __restrict__ zlist, int nx, int n_yt,
+                                                      unsigned* __restrict__ hdr, unsigned* __restrict__ units) {
+    __shared__ int part[32];
+    __shared__ int base;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    const int c = (int)hdr[1];
+    const int n_cols = n_yt * ((nx + c - 1) / c);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int c0 = 0; c0 < n_cols; c0 += 1024) {
+        const int col = c0 + threadIdx.x;
+        const int nb = col < n_cols ? (zlist[col] + 7) / 8 : 0;
+        int v = nb;  // inclusive scan within the warp
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += t;
+        }
+        if (lane == 31) part[w] = v;
+        __syncthreads();
+        if (w == 0) {
+            int x = part[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += t;
+            }
+            part[lane] = x;
+        }
+        __syncthreads();
+        const int excl = base + (w > 0 ? part[w - 1] : 0) + v - nb;
+        for (int b = 0; b < nb; ++b) units[excl + b] = ((unsigned)col << 5) | (unsigned)b;
+        __syncthreads();
+        if (threadIdx.x == 1023) base = excl + nb;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) hdr[0] = (unsigned)base;
+}
+
+// one step over the unit list: a wave of CTAs, CTA b runs units b, b + gridDim.x, ...
+__global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_c(const float* __restrict__ C, float* __restrict__ Cn,
+                                                                 const uint8_t* __restrict__ M, int nx, int ny,
+                                                                 int nz, int mz, const __grid_constant__ PlumeTab k,
+                                                                 const int* __restrict__ zlimit,
+                                                                 const uint8_t* __restrict__ zlist,
+                                                                 const unsigned* __restrict__ hdr,
+                                                                 const unsigned* __restrict__ units, int n_yt) {
+    __shared__ float w0s[64];
+    if (threadIdx.x < 64) w0s[threadIdx.x] = k.w0eff[threadIdx.x];
+    __syncthreads();
+    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
+    const int nu = (int)__ldg(&hdr[0]);
+    const int xc = (int)__ldg(&hdr[1]);
+    const int n_cols = n_yt * ((nx + xc - 1) / xc);
+    for (int u = blockIdx.x; u < nu; u += gridDim.x) {
+        const unsigned v = __ldg(&units[u]);
+        const int col = (int)(v >> 5);
+        const int xch = col / n_yt;
+        plume_direct_unit(C, Cn, M, nx, ny, nz, mz, xc, k, zl, zlist, n_cols, col, col - xch * n_yt, xch,
+                          (int)(v & 31u), w0s);
     }
 }
 
@@ -656,7 +835,7 @@ bool plume_resident_active(const BdPlumeParams* p) {
 
 // per-CTA step flags of the resident kernel, after the z lists in the plume scratch buffer
 static unsigned* resident_flags(uint8_t* mask, int nx, int ny, int nz) {
-    return reinterpret_cast<unsigned*>(mask + plume_zlist_offset(nx, ny, nz) + plume_zlist_bytes(nx, ny, nz));
+    return reinterpret_cast<unsigned*>(mask + plume_flags_offset(nx, ny, nz));
 }
 
 int plume_policy_steps(const BdPlumeParams* p, int* n_steps, float* dt_step, float* decay_step) {
@@ -689,6 +868,22 @@ int plume_policy_steps(const BdPlumeParams* p, int* n_steps, float* dt_step, flo
         return fail(BD_ERR_INVALID_ARG, "unknown plume dt policy %d", p->dt_policy);
     }
     return BD_OK;
+}
+
+// One wave of the compact step kernel on the current device: resident CTAs per SM x SMs (cached).
+static int compact_slots() {
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) dev = 0;
+    const int d = dev < 64 ? dev : 63;
+    int v = cache[d].load();
+    if (v > 0) return v;
+    int nsm = 0, per = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_plume_direct_c, 8 * PD_BY, 0);
+    v = std::max(1, nsm) * std::max(1, per);
+    cache[d].store(v);
+    return v;
 }
 
 // A plume stage: n_substeps x (steps per substep) FTCS steps on the ping-pong pair (Ca, Cb), the
@@ -746,6 +941,29 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
         }
     }
     const bool vec = nz % 4 == 0;  // the direct kernels move float4 groups
+    if (kernel == BD_PLUME_KERNEL_COMPACT && vec && (nz + 3) / 4 <= 255) {
+        const int n_yt = (ny + PD_BY - 1) / PD_BY;
+        unsigned* hdr = reinterpret_cast<unsigned*>(mask + plume_units_offset(nx, ny, nz));
+        unsigned* bits = hdr + kPlumeHdrWords;
+        unsigned* units = bits + (size_t)nx * n_yt * kPlumeBitWords;
+        uint8_t* zlist = mask + plume_zlist_offset(nx, ny, nz);
+        const int slots = compact_slots();
+        k_plume_planebits<<<dim3(n_yt, nx), 256, 0, st>>>(mask, nx, ny, nz, mz, zl, bits);
+        k_plume_unit_counts<<<kPlumeXcMax - kPlumeXcMin + 1, 1024, 0, st>>>(bits, nx, n_yt, (nz + 3) / 4, hdr);
+        k_plume_pick_xc<<<1, 32, 0, st>>>(hdr, slots + slots * 3 / 100);
+        k_plume_zlist_bits<<<dim3(n_yt, (nx + kPlumeXcMin - 1) / kPlumeXcMin), 256, 0, st>>>(bits, nx, nz, hdr, zlist);
+        k_plume_units<<<1, 1024, 0, st>>>(zlist, nx, n_yt, hdr, units);
+        BD_CHECK_LAUNCH("k_plume_units");
+        for (long long s = 0; s < total; ++s) {
+            const float* in = (s & 1) ? Cb : Ca;
+            float* out = (s & 1) ? Ca : Cb;
+            k_plume_direct_c<<<slots, 8 * PD_BY, 0, st>>>(in, out, mask, nx, ny, nz, mz, tab, zl, zlist, hdr, units,
+                                                           n_yt);
+        }
+        BD_CHECK_LAUNCH("k_plume_direct_c");
+        if (in_b) *in_b = (int)(total & 1);
+        return BD_OK;
+    }
     const int xc = tune_value(BD_TUNE_PLUME_XC);
     const dim3 dgrid((nz + PL_BZ - 1) / PL_BZ, (ny + PD_BY - 1) / PD_BY, (nx + xc - 1) / xc);
     // live z groups per direct-kernel column, from this stage's mask

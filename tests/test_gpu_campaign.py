@@ -34,7 +34,7 @@ def test_knob_validation(gpu, restore_knobs):
         _knob(_lib.TUNE_STENCIL_XC, 0)
     with pytest.raises(ValueError):
         _knob(_lib.TUNE_MC_BLOCKS_PER_SM, 17)
-    for bad in (0, 3, 6):
+    for bad in (0, 3, 7):
         with pytest.raises(ValueError):
             _knob(_lib.TUNE_PLUME_KERNEL, bad)
     with pytest.raises(ValueError):
@@ -66,7 +66,7 @@ def test_launch_shapes_leave_results_bit_identical(gpu, restore_knobs):
 def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
     """Every plume kernel gives the same bits: the resident kernel (one launch per stage, tiles
     kept in shared memory, halos swapped between CTAs; z >= 128 updated from global memory) and the
-    direct kernel (several x-chunk lengths), through the context API (arbitrary values in non-void
+    direct kernel in both unit orders (several x-chunk lengths), through the context API (arbitrary values in non-void
     voxels, ragged y tiles, scattered void, a partly filled last z tile, columns deeper than the
     shared-memory part) and through the engine (void z-limit, partly void voxel groups at the crater
     walls, bulk-void fast path)."""
@@ -87,7 +87,7 @@ def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
         C0 = (rng.uniform(0, 1, shape) * vd).astype(np.float32)
         z = np.zeros(shape)
         fields = []
-        for kern, xc in ((5, 4), (4, 2), (4, 1), (4, 3), (4, 4)):
+        for kern, xc in ((5, 4), (4, 2), (4, 1), (4, 3), (4, 4), (6, 4)):
             _knob(_lib.TUNE_PLUME_KERNEL, kern)
             _knob(_lib.TUNE_PLUME_XC, xc)
             ctx = gpu.MetalAblationContext(*shape, 0.03, 0.025, 0.02, 1e-5, 0.0, 20.0, 100.0, 300.0,
@@ -102,7 +102,7 @@ def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
         assert np.any(fields[0] != C0)
     inst = _small(22)                                  # 2940 nm, 80 W: a crater opens
     runs = []
-    for kern in (5, 4):
+    for kern in (5, 4, 6):
         _knob(_lib.TUNE_PLUME_KERNEL, kern)
         camp = campaign.Campaign([inst])
         camp.run(14, sync_every=14)
@@ -169,9 +169,16 @@ def test_autotune_sets_the_fastest_candidates(gpu, restore_knobs):
     from bug_defense_b200 import _lib, campaign
     res = campaign.autotune(_small(4), epochs_per_trial=2,
                             candidates={_lib.TUNE_MC_BLOCKS_PER_SM: [2, 4], _lib.TUNE_STENCIL_XC: [4, 8],
-                                        _lib.TUNE_PLUME_KERNEL: [4, 5], _lib.TUNE_PLUME_XC: [2, 4]})
-    for name, knob in (("mc_ctas_per_sm", _lib.TUNE_MC_BLOCKS_PER_SM), ("stencil_xc", _lib.TUNE_STENCIL_XC),
-                       ("plume_kernel", _lib.TUNE_PLUME_KERNEL), ("plume_xc", _lib.TUNE_PLUME_XC)):
+                                        _lib.TUNE_PLUME_KERNEL: [4, 6, 5], _lib.TUNE_PLUME_XC: [2, 4]})
+    for name, knob in (("mc_ctas_per_sm", _lib.TUNE_MC_BLOCKS_PER_SM), ("stencil_xc", _lib.TUNE_STENCIL_XC)):
         trials = res["trials"][name]
         assert [v for v, _ in trials] == sorted(v for v, _ in trials) and all(t > 0 for _, t in trials)
         assert res[name] == min(trials, key=lambda t: t[1])[0] == _knob(knob)
+    # the plume kernel and the direct kernel's x-planes are searched together; the compact kernel
+    # picks its x-planes per stage and the resident kernel has none
+    plume = res["trials"]["plume"]
+    assert [(k, x) for k, x, _ in plume] == [(4, 2), (4, 4), (6, None), (5, None)]
+    assert all(t > 0 for _, _, t in plume)
+    k, x, _ = min(plume, key=lambda t: t[2])
+    assert res["plume_kernel"] == k == _knob(_lib.TUNE_PLUME_KERNEL)
+    assert res["plume_xc"] == _knob(_lib.TUNE_PLUME_XC) and (x is None or res["plume_xc"] == x)
