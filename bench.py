@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--plume-kernel", type=int, default=None, choices=[4, 5, 6],
                     help="plume kernel to use (4 direct, 5 resident, 6 direct over a compact unit list) instead of "
                          "the autotuner's choice")
+    ap.add_argument("--batch-plume", action="store_true",
+                    help="campaign: run the instances' plume stages as one batched stage (one launch per step)")
     ap.add_argument("--workload", default="coupled", choices=["coupled", "campaign"],
                     help="coupled: the headline run; campaign: 24 wavelength x power x pulse instances at once")
     return ap.parse_args()
@@ -535,7 +537,7 @@ def campaign_main(args):
     t0 = time.perf_counter()
     tuned = campaign.autotune(insts[0])
     t_tune = time.perf_counter() - t0
-    camp = campaign.Campaign(insts)
+    camp = campaign.Campaign(insts, batch_plume=bool(args.batch_plume))
     camp.enqueue(args.warmup)
     camp.diagnostics()
     K = int(args.steps)
@@ -567,7 +569,9 @@ def campaign_main(args):
            "dtype": "f32 (FP64 ledgers)", "data": "synthetic (seeded, reference config shapes)",
            "config": {"workload": "campaign: 8 wavelengths x 3 powers, pulse U(50, 400) ms, 200x200x192 @ 15 um, "
                                   "150k photons per laser epoch", "instances": n_inst,
-                      "parallelism": f"instances split over {world} rank(s)"},
+                      "parallelism": f"instances split over {world} rank(s)",
+                      "plume_stage": ("batched: one launch per FTCS step over every instance's live units"
+                                      if camp.batch is not None else "one stage per instance")},
            "autotune": {k: v for k, v in tuned.items()}, "autotune_s": round(t_tune, 1),
            "setup_s": round(camp.setup_s, 1),
            "void_voxels_end": [int(d["n_void"]) for d in diags],

@@ -102,6 +102,7 @@ FLAG_NEWLY = 0x08
 EPOCH_SKIP_MC = 0x1
 EPOCH_NO_GRAPH = 0x2
 EPOCH_SERIAL_PLUME = 0x4
+EPOCH_EXTERNAL_PLUME = 0x8
 
 
 class GridRef(Structure):
@@ -213,6 +214,10 @@ _SIGNATURES = {
     "bd_engine_destroy": (c_int, [c_void_p]),
     "bd_engine_step_epoch": (c_int, [c_void_p, c_float, c_int, c_void_p]),
     "bd_engine_epoch_end": (c_int, [c_void_p, c_void_p]),
+    "bd_engine_epoch_finish": (c_int, [c_void_p, c_void_p]),
+    "bd_plume_batch_create": (c_int, [ctypes.POINTER(c_void_p), c_int, ctypes.POINTER(c_void_p)]),
+    "bd_plume_batch_run": (c_int, [c_void_p, c_void_p]),
+    "bd_plume_batch_destroy": (c_int, [c_void_p]),
     "bd_engine_read_diag": (c_int, [c_void_p, POINTER(EpochDiag), c_void_p]),
     "bd_engine_set_time": (c_int, [c_void_p, c_double, c_int64, c_void_p]),
     "bd_engine_set_mc": (c_int, [c_void_p, POINTER(McParams)]),

@@ -244,10 +244,15 @@ class Campaign:
 
     With the resident plume kernel (BD_PLUME_KERNEL_RESIDENT) each instance's plume stage occupies every SM, so
     the instances share one CUDA stream: two resident stages on concurrent streams could each hold
-    part of the GPU while waiting for the rest. With the per-step plume kernel every instance gets
-    its own stream and the instances' stages overlap."""
+    part of the GPU while waiting for the rest. Otherwise every instance gets its own stream and
+    runs its own plume stage beside its own MC and substeps. With `batch_plume` the instances' plume
+    stages instead run as one batched stage (bd_plume_batch_run: one launch per FTCS step over the
+    live units of every instance still stepping) on a stream of its own, beside the instances' MC and
+    substeps, and each instance's epoch end waits for it. Same results; measured slower on the
+    24-instance campaign (the batched stage streams every instance's field through L2 each step,
+    where an instance's own stage keeps its field resident), so it is off by default."""
 
-    def __init__(self, instances, device=None, use_graphs: bool = True, log=None):
+    def __init__(self, instances, device=None, use_graphs: bool = True, log=None, batch_plume: bool = False):
         import torch
         from . import _lib
         self.instances = list(instances)
@@ -267,16 +272,61 @@ class Campaign:
             if log:
                 log(f"instance {inst['index']}: {inst['wavelength_nm']:.0f} nm, {inst['power']:.0f} W, "
                     f"pulse {inst['pulse_ms']:.0f} ms")
+        self.batch = None
+        if batch_plume and not self.shared_stream and len(self.engines) <= 32 and use_graphs:
+            n = len(self.engines)
+            arr = (ctypes.c_void_p * n)(*[e._handle for e in self.engines])
+            h = ctypes.c_void_p()
+            _lib.call("bd_plume_batch_create", arr, n, ctypes.byref(h))
+            self.batch = h
+            dev = self.engines[0].dev
+            self.plume_stream = torch.cuda.Stream(device=dev, priority=-1)
+            self.ev_prev = [torch.cuda.Event() for _ in self.engines]
+            self.ev_plume = torch.cuda.Event()
         self.setup_s = time.perf_counter() - t0
         self.epoch = 0
 
+    def close(self):
+        """Release the batched plume stage (the engines stay usable)."""
+        from . import _lib
+        if self.batch is not None:
+            import torch
+            torch.cuda.synchronize(self.engines[0].dev)
+            _lib.call("bd_plume_batch_destroy", self.batch)
+            self.batch = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
     def enqueue(self, n_epochs: int):
         import torch
+        from . import _lib
         for _ in range(int(n_epochs)):
-            for eng, st in zip(self.engines, self.streams):
-                with torch.cuda.stream(st):
-                    eng.power = eng.laser_power if self.epoch < eng.epochs_on else 0.0
-                    eng._enqueue(0)
+            if self.batch is None:
+                for eng, st in zip(self.engines, self.streams):
+                    with torch.cuda.stream(st):
+                        eng.power = eng.laser_power if self.epoch < eng.epochs_on else 0.0
+                        eng._enqueue(0)
+            else:
+                # the batched plume stage starts once every instance's previous epoch has ended and
+                # runs beside their MC and substeps; each instance's epoch end waits for it
+                for eng, st, ev in zip(self.engines, self.streams, self.ev_prev):
+                    ev.record(st)
+                    with torch.cuda.stream(st):
+                        eng.power = eng.laser_power if self.epoch < eng.epochs_on else 0.0
+                        eng._enqueue(_lib.EPOCH_EXTERNAL_PLUME)
+                for ev in self.ev_prev:
+                    self.plume_stream.wait_event(ev)
+                with torch.cuda.stream(self.plume_stream):
+                    _lib.call("bd_plume_batch_run", self.batch, _lib.stream_ptr())
+                self.ev_plume.record(self.plume_stream)
+                for eng, st in zip(self.engines, self.streams):
+                    st.wait_event(self.ev_plume)
+                    with torch.cuda.stream(st):
+                        _lib.call("bd_engine_epoch_finish", eng._handle, _lib.stream_ptr())
             self.epoch += 1
 
     def diagnostics(self):

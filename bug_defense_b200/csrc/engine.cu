@@ -291,7 +291,8 @@ extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void*
 
     const bool laser = power > 0.0f;
     int rc = BD_OK;
-    const bool plume = d.n_substeps > 0 && d.has_plume_transport;
+    const bool external = (options & BD_EPOCH_EXTERNAL_PLUME) != 0;
+    const bool plume = d.n_substeps > 0 && d.has_plume_transport && !external;
     const bool conc = plume && e->side && !(options & BD_EPOCH_SERIAL_PLUME) && !plume_resident_active(&d.plume);
     auto plume_stage = [&](cudaStream_t on) -> int {
         return run_stage(e, e->g_plume, &d.plume, sizeof(d.plume), graphs, on, [&](cudaStream_t s) -> int {
@@ -369,6 +370,7 @@ extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void*
         }
         mark(e, st, 2);
     }
+    if (external) return BD_OK;  // the caller runs the plume stage, then bd_engine_epoch_finish
     rc = run_stage(e, e->g_end, &e->pa, sizeof(e->pa), graphs, st, [&](cudaStream_t s) -> int {
         return phase_launch(e->pa, BD_PHASE_FULL, s);
     });
@@ -456,6 +458,113 @@ extern "C" int bd_engine_timing_read(BdEngine* e, double* stage_ms, int64_t* epo
         }
         for (int q = 0; q < 4; ++q) stage_ms[q] += ms[q];
     }
+    return BD_OK;
+}
+
+extern "C" int bd_engine_epoch_finish(BdEngine* e, void* stream) {
+    BD_REQUIRE(e != nullptr, "bd_engine_epoch_finish: NULL engine");
+    cudaStream_t st = as_stream(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    BD_CUDA(cudaStreamIsCapturing(st, &cap));
+    const bool graphs = cap == cudaStreamCaptureStatusNone;
+    int rc = run_stage(e, e->g_end, &e->pa, sizeof(e->pa), graphs, st, [&](cudaStream_t s) -> int {
+        return phase_launch(e->pa, BD_PHASE_FULL, s);
+    });
+    if (rc == BD_OK && e->timed) cudaEventRecord(e->ev[3], st);
+    return rc;
+}
+
+// Several engines' plume stages as one batched stage (one launch per FTCS step for all of them).
+struct BdPlumeBatch {
+    std::vector<BdEngine*> eng;
+    std::vector<bd::PlumeInstHost> host;
+    std::vector<int> order;
+    void* dev = nullptr;             // device descriptors, ranked by step count
+    unsigned* units = nullptr;
+    long long max_steps = 0;
+    cudaStream_t cap_stream = nullptr;
+    StageGraph g;
+};
+
+extern "C" int bd_plume_batch_create(BdEngine* const* engines, int n, BdPlumeBatch** out) {
+    BD_REQUIRE(engines && out, "bd_plume_batch_create: NULL argument");
+    BD_REQUIRE(n >= 1 && n <= 32, "bd_plume_batch_create: 1..32 engines, got %d", n);
+    const BdEngine* e0 = engines[0];
+    BD_REQUIRE(e0 != nullptr, "bd_plume_batch_create: NULL engine");
+    const BdPlumeParams& p0 = e0->d.plume;
+    for (int i = 0; i < n; ++i) {
+        const BdEngine* e = engines[i];
+        BD_REQUIRE(e != nullptr, "bd_plume_batch_create: engine %d is NULL", i);
+        BD_REQUIRE(e->d.has_plume_transport && e->d.n_substeps > 0,
+                   "bd_plume_batch_create: engine %d has no plume transport", i);
+        const BdPlumeParams& p = e->d.plume;
+        BD_REQUIRE(p.nx == p0.nx && p.ny == p0.ny && p.nz == p0.nz && p.dx == p0.dx && p.dy == p0.dy && p.dz == p0.dz,
+                   "bd_plume_batch_create: engine %d has another grid", i);
+        BD_REQUIRE(p.nz % 4 == 0 && p.nz <= 1020, "bd_plume_batch_create: needs nz %% 4 == 0 and nz <= 1020");
+    }
+    BdPlumeBatch* b = new BdPlumeBatch();
+    b->order.resize(n);
+    for (int i = 0; i < n; ++i) {
+        BdEngine* e = engines[i];
+        b->eng.push_back(e);
+        b->host.push_back(bd::PlumeInstHost{e->d.phase.plume, e->d.plume_alt, e->plume_mask, e->d.phase.flags,
+                                            &e->dyn->void_zlimit, &e->d.plume, e->d.n_substeps});
+    }
+    cudaError_t err = cudaMalloc(&b->dev, bd::plume_batch_desc_bytes(n));
+    if (err == cudaSuccess)
+        err = cudaMalloc((void**)&b->units, sizeof(unsigned) * bd::plume_batch_units_words(n, p0.nx, p0.ny, p0.nz));
+    if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
+    int rc = err == cudaSuccess ? BD_OK : cuda_status(err, "bd_plume_batch_create");
+    if (rc == BD_OK) rc = bd::plume_batch_prepare(n, b->host.data(), b->dev, b->order.data(), &b->max_steps);
+    if (rc != BD_OK) {
+        if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+        cudaFree(b->dev);
+        cudaFree(b->units);
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return BD_OK;
+}
+
+extern "C" int bd_plume_batch_run(BdPlumeBatch* b, void* stream) {
+    BD_REQUIRE(b != nullptr, "bd_plume_batch_run: NULL batch");
+    cudaStream_t st = as_stream(stream);
+    const int n = (int)b->eng.size();
+    auto enqueue = [&](cudaStream_t s) -> int {
+        return bd::plume_batch_launch(n, b->host.data(), b->order.data(), b->dev, b->max_steps, b->units, s);
+    };
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    BD_CUDA(cudaStreamIsCapturing(st, &cap));
+    if (cap != cudaStreamCaptureStatusNone) return enqueue(st);
+    // a captured graph, re-captured when a launch-shape knob changed
+    if (!b->g.exec || b->g.tune_gen != bd::tune_generation()) {
+        graph_reset(b->g);
+        cudaGraph_t graph = nullptr;
+        BD_CUDA(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue(b->cap_stream);
+        cudaError_t ce = cudaStreamEndCapture(b->cap_stream, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (ce != cudaSuccess) return cuda_status(ce, "bd_plume_batch_run: capture");
+        ce = cudaGraphInstantiate(&b->g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return cuda_status(ce, "bd_plume_batch_run: instantiate");
+        b->g.tune_gen = bd::tune_generation();
+    }
+    BD_CUDA(cudaGraphLaunch(b->g.exec, st));
+    return BD_OK;
+}
+
+extern "C" int bd_plume_batch_destroy(BdPlumeBatch* b) {
+    if (!b) return BD_OK;
+    graph_reset(b->g);
+    if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+    cudaFree(b->dev);
+    cudaFree(b->units);
+    delete b;
     return BD_OK;
 }
 

@@ -59,6 +59,27 @@ int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, floa
 int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
                  cudaStream_t st, const int* zlimit, int full_first, uint8_t* mask, int* err);
 int plume_policy_steps(const BdPlumeParams* p, int* n_steps, float* dt_step, float* decay_step);
+// One instance of a batched plume stage (several engines' plume stages in one launch per step).
+struct PlumeTab;
+struct PlumeInstHost {
+    float* Ca;               // the field at the start of the stage
+    float* Cb;               // the other ping-pong buffer
+    uint8_t* mask;           // the instance's neighbourhood bytes + z lists (plume_mask_bytes)
+    const uint8_t* flags;    // voxel flags (void bit)
+    const int* zlimit;       // void z-limit on the device
+    const BdPlumeParams* params;
+    int n_substeps;
+};
+// Plume stages of n instances of one grid (their diffusivities, and so their weights and step
+// counts, may differ): per instance its mask and z lists, then one list of the live (instance,
+// column, band) units, then one launch per FTCS step covering every instance still stepping.
+// plume_batch_prepare fills the device descriptors (`dev`, plume_batch_desc_bytes(n) bytes) and
+// orders the instances by step count (order[r] = instance of rank r); the launch enqueues a stage.
+size_t plume_batch_desc_bytes(int n);
+size_t plume_batch_units_words(int n, int nx, int ny, int nz);
+int plume_batch_prepare(int n, const PlumeInstHost* insts, void* dev, int* order, long long* max_steps);
+int plume_batch_launch(int n, const PlumeInstHost* insts, const int* order, const void* dev, long long max_steps,
+                       unsigned* units, cudaStream_t st);
 // true when plume stages of this grid run as one resident launch (its CTAs then occupy every SM for
 // the stage, so the engine runs the stage in line rather than beside MC and the substeps)
 bool plume_resident_active(const BdPlumeParams* p);

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <vector>
 #include <cmath>
 
 namespace bd {
@@ -987,6 +988,218 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     }
     BD_CHECK_LAUNCH("k_plume_step");
     if (in_b) *in_b = (int)(total & 1);
+    return BD_OK;
+}
+
+// ---- batched stages: several instances' plume steps in one launch per step ------------------
+// The instances may differ in diffusivity, so each carries its own weights and step count. They
+// are ranked by step count (rank 0 steps longest); a unit of rank r is (r << 27) | (column << 5) |
+// band, and the unit list is in (rank, column) order, so the units of step s are a prefix of it:
+// those of the ranks that still step. The header holds the unit count [0] and, at [16 + r], the
+// units of ranks 0..r; the units follow at word 64.
+struct PlumeInstDev {
+    float* Ca;
+    float* Cb;
+    const uint8_t* mask;
+    const int* zlimit;
+    long long steps;  // FTCS steps of the stage (steps per substep x substeps)
+    PlumeTab tab;
+};
+constexpr int kBatchHdrWords = 64;
+
+__global__ void __launch_bounds__(1024) k_plume_batch_units(const PlumeInstDev* __restrict__ insts, int n,
+                                                            int n_cols, size_t zoff, unsigned* __restrict__ hdr) {
+    __shared__ int part[32];
+    __shared__ int base;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    unsigned* units = hdr + kBatchHdrWords;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int total = n * n_cols;
+    for (int c0 = 0; c0 < total; c0 += 1024) {
+        const int q = c0 + threadIdx.x;
+        int nb = 0, r = 0, col = 0;
+        if (q < total) {
+            r = q / n_cols;
+            col = q - r * n_cols;
+            nb = (insts[r].mask[zoff + col] + 7) / 8;
+        }
+        int v = nb;  // inclusive scan within the warp
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += t;
+        }
+        if (lane == 31) part[w] = v;
+        __syncthreads();
+        if (w == 0) {
+            int x = part[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += t;
+            }
+            part[lane] = x;
+        }
+        __syncthreads();
+        const int excl = base + (w > 0 ? part[w - 1] : 0) + v - nb;
+        for (int b = 0; b < nb; ++b) units[excl + b] = ((unsigned)r << 27) | ((unsigned)col << 5) | (unsigned)b;
+        if (q < total && col == n_cols - 1) hdr[16 + r] = (unsigned)(excl + nb);  // units of ranks 0..r
+        __syncthreads();
+        if (threadIdx.x == 1023) base = excl + nb;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) hdr[0] = (unsigned)base;
+}
+
+// step s of every instance that still steps: a wave of CTAs looping over a prefix of the units. At
+// the start every CTA copies each instance's buffers, void z-limit and weights into shared memory,
+// so a unit costs the same dependent loads as one of the compact kernel.
+constexpr int kBatchMax = 32;
+__global__ void __launch_bounds__(8 * PD_BY, 8) k_plume_direct_b(const PlumeInstDev* __restrict__ insts, int n,
+                                                                 long long s, int nx, int ny, int nz, int mz, int xc,
+                                                                 size_t zoff, const unsigned* __restrict__ hdr,
+                                                                 int n_yt) {
+    __shared__ float w0s[kBatchMax][64];
+    __shared__ float sc[kBatchMax][6];  // wx, wy, wb, wt, decay, decays
+    __shared__ const float* cin[kBatchMax];
+    __shared__ float* cout[kBatchMax];
+    __shared__ const uint8_t* msk[kBatchMax];
+    __shared__ int zls[kBatchMax];
+    __shared__ int nu_s;
+    const int odd = (int)(s & 1);
+    for (int q = threadIdx.x; q < n * 64; q += blockDim.x) w0s[q >> 6][q & 63] = insts[q >> 6].tab.w0eff[q & 63];
+    if (threadIdx.x < n) {
+        const PlumeInstDev& in = insts[threadIdx.x];
+        float* t = sc[threadIdx.x];
+        t[0] = in.tab.wx;
+        t[1] = in.tab.wy;
+        t[2] = in.tab.wb;
+        t[3] = in.tab.wt;
+        t[4] = in.tab.decay;
+        t[5] = in.tab.decays ? 1.0f : 0.0f;
+        cin[threadIdx.x] = odd ? in.Cb : in.Ca;
+        cout[threadIdx.x] = odd ? in.Ca : in.Cb;
+        msk[threadIdx.x] = in.mask;
+        zls[threadIdx.x] = in.zlimit ? min(max(*in.zlimit, 0), nz) : nz;
+    }
+    if (threadIdx.x == 0) {
+        int r = 0;
+        while (r < n && insts[r].steps > s) ++r;
+        nu_s = r > 0 ? (int)hdr[16 + r - 1] : 0;
+    }
+    __syncthreads();
+    const int nu = nu_s;
+    const unsigned* units = hdr + kBatchHdrWords;
+    const int n_cols = n_yt * ((nx + xc - 1) / xc);
+    for (int u = blockIdx.x; u < nu; u += gridDim.x) {
+        const unsigned v = __ldg(&units[u]);
+        const int ri = (int)(v >> 27);
+        PlumeTab kt;
+        kt.wx = sc[ri][0];
+        kt.wy = sc[ri][1];
+        kt.wb = sc[ri][2];
+        kt.wt = sc[ri][3];
+        kt.decay = sc[ri][4];
+        kt.decays = sc[ri][5] != 0.0f;
+        const int col = (int)((v >> 5) & 0x3FFFFFu);
+        const int xch = col / n_yt;
+        const uint8_t* M = msk[ri];
+        plume_direct_unit(cin[ri], cout[ri], M, nx, ny, nz, mz, xc, kt, zls[ri], M + zoff, n_cols, col,
+                          col - xch * n_yt, xch, (int)(v & 31u), w0s[ri]);
+    }
+}
+
+size_t plume_batch_desc_bytes(int n) { return sizeof(PlumeInstDev) * (size_t)n; }
+
+size_t plume_batch_units_words(int n, int nx, int ny, int nz) {
+    const size_t cols = (size_t)nx * ((ny + PD_BY - 1) / PD_BY);
+    const size_t bands = ((size_t)(nz + 3) / 4 + 7) / 8;
+    return kBatchHdrWords + (size_t)n * cols * bands;
+}
+
+static int batch_steps(const PlumeInstHost& q, long long* total, PlumeTab* tab) {
+    int steps;
+    float dtp, decay;
+    int rc = plume_policy_steps(q.params, &steps, &dtp, &decay);
+    if (rc) return rc;
+    const BdPlumeParams* p = q.params;
+    PlumeConst c;
+    c.dxy_x = p->D_xy / (p->dx * p->dx);
+    c.dxy_y = p->D_xy / (p->dy * p->dy);
+    c.dz_z = p->D_z / (p->dz * p->dz);
+    c.vz_over_dz = p->vz > 0.0f ? p->vz / p->dz : 0.0f;
+    c.dtp = dtp;
+    c.decay = decay;
+    if (tab) *tab = make_plume_tab(c);
+    *total = (long long)steps * q.n_substeps;
+    return BD_OK;
+}
+
+int plume_batch_prepare(int n, const PlumeInstHost* insts, void* dev, int* order, long long* max_steps) {
+    BD_REQUIRE(n >= 1 && n <= kBatchMax, "plume batch: 1..%d instances, got %d", kBatchMax, n);
+    std::vector<long long> total(n);
+    std::vector<PlumeTab> tabs(n);
+    for (int i = 0; i < n; ++i) {
+        int rc = batch_steps(insts[i], &total[i], &tabs[i]);
+        if (rc) return rc;
+        order[i] = i;
+    }
+    std::stable_sort(order, order + n, [&](int a, int b) { return total[a] > total[b]; });
+    std::vector<PlumeInstDev> h(n);
+    for (int r = 0; r < n; ++r) {
+        const PlumeInstHost& q = insts[order[r]];
+        h[r].Ca = q.Ca;
+        h[r].Cb = q.Cb;
+        h[r].mask = q.mask;
+        h[r].zlimit = q.zlimit;
+        h[r].steps = total[order[r]];
+        h[r].tab = tabs[order[r]];
+    }
+    *max_steps = total[order[0]];
+    BD_CUDA(cudaMemcpy(dev, h.data(), sizeof(PlumeInstDev) * n, cudaMemcpyHostToDevice));
+    return BD_OK;
+}
+
+int plume_batch_launch(int n, const PlumeInstHost* insts, const int* order, const void* dev, long long max_steps,
+                       unsigned* units, cudaStream_t st) {
+    const BdPlumeParams* p = insts[0].params;
+    const int nx = p->nx, ny = p->ny, nz = p->nz;
+    const int mz = plume_mask_pitch(nz);
+    const int xc = tune_value(BD_TUNE_PLUME_XC);
+    const int n_yt = (ny + PD_BY - 1) / PD_BY, n_xch = (nx + xc - 1) / xc;
+    const size_t zoff = plume_zlist_offset(nx, ny, nz);
+    for (int i = 0; i < n; ++i) {
+        const PlumeInstHost& q = insts[i];
+        k_plume_mask<<<dim3((ny + PM_TY - 1) / PM_TY, nx), dim3(PM_TZ, PM_TY), 0, st>>>(nx, ny, nz, mz, q.flags, q.mask,
+                                                                                       q.zlimit);
+        k_plume_zlist<<<dim3(n_yt, n_xch), 256, 0, st>>>(q.mask, nx, ny, nz, mz, xc, q.zlimit, q.mask + zoff);
+    }
+    BD_CHECK_LAUNCH("k_plume_zlist");
+    const PlumeInstDev* d = static_cast<const PlumeInstDev*>(dev);
+    k_plume_batch_units<<<1, 1024, 0, st>>>(d, n, n_yt * n_xch, zoff, units);
+    BD_CHECK_LAUNCH("k_plume_batch_units");
+    static std::atomic<int> per_sm{0};  // resident CTAs per SM of the batched step kernel
+    if (per_sm.load() == 0) {
+        int v = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_plume_direct_b, 8 * PD_BY, 0);
+        per_sm.store(std::max(1, v));
+    }
+    int dev_id = 0, nsm = 0;
+    cudaGetDevice(&dev_id);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev_id);
+    const int slots = std::max(1, nsm) * per_sm.load();
+    for (long long s = 0; s < max_steps; ++s)
+        k_plume_direct_b<<<slots, 8 * PD_BY, 0, st>>>(d, n, s, nx, ny, nz, mz, xc, zoff, units, n_yt);
+    BD_CHECK_LAUNCH("k_plume_direct_b");
+    // an instance whose step count is odd ends in its Cb buffer
+    const long long nv = (long long)nx * ny * nz;
+    for (int i = 0; i < n; ++i) {
+        long long total = 0;
+        int rc = batch_steps(insts[i], &total, nullptr);
+        if (rc) return rc;
+        if (total & 1)
+            BD_CUDA(cudaMemcpyAsync(insts[i].Ca, insts[i].Cb, sizeof(float) * nv, cudaMemcpyDeviceToDevice, st));
+    }
+    (void)order;
     return BD_OK;
 }
 }  // namespace bd

@@ -290,6 +290,9 @@ typedef struct BdEpochDiag {
 #define BD_EPOCH_NO_GRAPH 0x2      /* launch the stages directly instead of as CUDA graphs  */
 #define BD_EPOCH_SERIAL_PLUME 0x4  /* run the plume stage after the substeps on the caller's stream
                                       instead of beside MC + substeps on the engine's plume stream */
+#define BD_EPOCH_EXTERNAL_PLUME 0x8 /* enqueue the epoch's start, MC and substeps only: the caller runs
+                                      the plume stage (bd_plume_batch_run) and then the epoch end
+                                      (bd_engine_epoch_finish)                                      */
 
 typedef struct BdEngine BdEngine;
 /* Replaces CoupledAblationEngine.__init__ device setup (coupled_ablation.py:184-407);
@@ -301,6 +304,21 @@ BD_API int bd_engine_destroy(BdEngine* e);
 BD_API int bd_engine_step_epoch(BdEngine* e, float power, int options, void* stream);
 /* Only the epoch-end update (phase, removal, breach, plume sync, MC properties). */
 BD_API int bd_engine_epoch_end(BdEngine* e, void* stream);
+/* The epoch end of an epoch enqueued with BD_EPOCH_EXTERNAL_PLUME (the stage bd_engine_step_epoch
+ * ends with otherwise); enqueue it after that epoch's plume stage. */
+BD_API int bd_engine_epoch_finish(BdEngine* e, void* stream);
+
+/* Batched plume stage: the plume stages of up to 32 engines of one grid and one set of plume
+ * parameters run as one launch per FTCS step over the live units of every engine (a campaign's
+ * instances; no reference counterpart: the reference runs its campaign as sequential processes,
+ * run_highres_knowledge_suite.py:633-654). The engines' epochs are enqueued with
+ * BD_EPOCH_EXTERNAL_PLUME; bd_plume_batch_run then advances every engine's plume field over one epoch
+ * (its results are those of each engine's own stage), after which each engine's epoch end is
+ * enqueued with bd_engine_epoch_finish. The stage runs as a CUDA graph captured on the first call. */
+typedef struct BdPlumeBatch BdPlumeBatch;
+BD_API int bd_plume_batch_create(BdEngine* const* engines, int n, BdPlumeBatch** out);
+BD_API int bd_plume_batch_run(BdPlumeBatch* b, void* stream);
+BD_API int bd_plume_batch_destroy(BdPlumeBatch* b);
 /* Synchronises `stream` and copies the diagnostics of the last epoch to the host. */
 BD_API int bd_engine_read_diag(BdEngine* e, BdEpochDiag* out, void* stream);
 BD_API int bd_engine_set_time(BdEngine* e, double t, int64_t epoch, void* stream);

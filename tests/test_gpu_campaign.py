@@ -146,23 +146,31 @@ def _small(index, photons=20_000):
     return dict(inst, n_photons=photons, pulse_ms=12.0)
 
 
-@pytest.mark.parametrize("kern", [4, 5], ids=["direct-streams", "resident-one-stream"])
-def test_concurrent_campaign_equals_instances_run_alone(gpu, restore_knobs, kern):
+@pytest.mark.parametrize("kern,batch", [(4, True), (4, False), (5, False)],
+                         ids=["batched-plume", "direct-streams", "resident-one-stream"])
+def test_concurrent_campaign_equals_instances_run_alone(gpu, restore_knobs, kern, batch):
+    """Instances run together give the bits of each instance run alone with its own plume stage:
+    with the batched plume stage (one launch per FTCS step over every instance's units), with each
+    instance's stages on its own stream, and with the resident kernel on one shared stream."""
     from bug_defense_b200 import _lib, campaign
     _knob(_lib.TUNE_PLUME_KERNEL, kern)
     insts = [_small(i) for i in (1, 10, 23)]           # 532, 1064 and 2940 nm
-    camp = campaign.Campaign(insts)
+    camp = campaign.Campaign(insts, batch_plume=batch)
     assert camp.shared_stream == (kern == _lib.PLUME_KERNEL_RESIDENT)
+    assert (camp.batch is not None) == batch
     camp.run(30, sync_every=10)
-    together = [(e.T.copy(), e.ablated.copy(), e.H_acc.copy()) for e in camp.engines]
-    for inst, (T, abl, H) in zip(insts, together):
-        solo = campaign.Campaign([inst])
+    together = [(e.T.copy(), e.ablated.copy(), e.H_acc.copy(), e.plume.raw.double().cpu().numpy())
+                for e in camp.engines]
+    camp.close()
+    for inst, (T, abl, H, C) in zip(insts, together):
+        solo = campaign.Campaign([inst], batch_plume=False)
         solo.run(30, sync_every=30)
         e = solo.engines[0]
         assert np.array_equal(e.T, T) and np.array_equal(e.ablated, abl) and np.array_equal(e.H_acc, H)
+        assert np.array_equal(e.plume.raw.double().cpu().numpy(), C)
     # the lasers did work: every instance heated up, the 2940 nm one ablated
-    assert all(float(T.max()) > 40.0 for T, _, _ in together)
-    assert together[2][1].sum() > together[0][1].sum()
+    assert all(float(T.max()) > 40.0 for T, _, _, _ in together)
+    assert together[2][1].sum() > together[0][1].sum() and np.any(together[2][3] > 0)
 
 
 def test_autotune_sets_the_fastest_candidates(gpu, restore_knobs):
