@@ -331,30 +331,32 @@ __device__ __forceinline__ void plume_direct_unit(const float* __restrict__ C, f
     const int ib = xch * xc, ie = min(nx, ib + xc);
     if (b0 >= cnt || ib >= ie) return;
     const int zg = threadIdx.x & 7;
-    const int g = b0 + zg < cnt ? (int)zlist[n_cols + (size_t)col * G + b0 + zg] : -2;
+    const int g = b0 + zg < cnt ? (int)zlist[n_cols + col * G + b0 + zg] : -2;
     const int gp = __shfl_up_sync(0xffffffffu, g, 1, 8);
     const int gn = __shfl_down_sync(0xffffffffu, g, 1, 8);
     const bool zb_lane = zg > 0 && gp == g - 1;  // the -z neighbour is the previous lane's last voxel
     const bool zt_lane = zg < 7 && gn == g + 1;  // the +z neighbour is the next lane's first voxel
-    const int j = yt * PD_BY + (threadIdx.x >> 3), z = 4 * max(g, 0);
+    const int j = yt * PD_BY + ((threadIdx.x & 127) >> 3), z = 4 * max(g, 0);
     const bool act = g >= 0 && zl - z > 0 && j < ny;
     const bool in = g >= 0 && j < ny && z < nz;
     const unsigned zkeep = zkeep_mask(zl, z);
-    const size_t plane = (size_t)ny * nz;
-    const size_t mplane = (size_t)ny * mz;
+    // 32-bit element offsets (grids have < 2^31 voxels); rows past the grid load nothing
+    const int plane = ny * nz, mplane = ny * mz;
+    const int jj = min(j, ny - 1);
+    int off = (ib * ny + jj) * nz + z;
+    int moff = (ib * ny + jj) * mz + z;
+    const bool ys = in && j > 0, yn = in && j + 1 < ny;
+    const bool ebl = !zb_lane && in && z > 0, etl = !zt_lane && in && z + 4 < nz;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    size_t idx = ((size_t)ib * ny + j) * nz + z;
-    const uint8_t* mp = M + ((size_t)ib * ny + j) * mz + z;
-    float4 cw = in && ib > 0 ? __ldg(reinterpret_cast<const float4*>(C + idx - plane)) : z4;
-    float4 cc = in ? __ldg(reinterpret_cast<const float4*>(C + idx)) : z4;
-    for (int i = ib; i < ie; ++i, idx += plane, mp += mplane) {
-        const unsigned mr = act ? (__ldg(reinterpret_cast<const unsigned*>(mp)) & zkeep) : 0u;
-        const float4 ce = in && i + 1 < nx ? __ldg(reinterpret_cast<const float4*>(C + idx + plane)) : z4;
-        const float4 cs = in && j > 0 ? __ldg(reinterpret_cast<const float4*>(C + idx - nz)) : z4;
-        const float4 cn = in && j + 1 < ny ? __ldg(reinterpret_cast<const float4*>(C + idx + nz)) : z4;
-        float eb = 0.0f, et = 0.0f;
-        if (!zb_lane && in && z > 0) eb = __ldg(C + idx - 1);
-        if (!zt_lane && in && z + 4 < nz) et = __ldg(C + idx + 4);
+    float4 cw = in && ib > 0 ? __ldg(reinterpret_cast<const float4*>(C + (off - plane))) : z4;
+    float4 cc = in ? __ldg(reinterpret_cast<const float4*>(C + off)) : z4;
+    for (int i = ib; i < ie; ++i, off += plane, moff += mplane) {
+        const unsigned mr = act ? (__ldg(reinterpret_cast<const unsigned*>(M + moff)) & zkeep) : 0u;
+        const float4 ce = in && i + 1 < nx ? __ldg(reinterpret_cast<const float4*>(C + (off + plane))) : z4;
+        const float4 cs = ys ? __ldg(reinterpret_cast<const float4*>(C + (off - nz))) : z4;
+        const float4 cn = yn ? __ldg(reinterpret_cast<const float4*>(C + (off + nz))) : z4;
+        const float eb = ebl ? __ldg(C + (off - 1)) : 0.0f;
+        const float et = etl ? __ldg(C + (off + 4)) : 0.0f;
         const unsigned vd = mr & 0x40404040u;
         if (__any_sync(0xffffffffu, act && vd)) {
             float zb = __shfl_up_sync(0xffffffffu, cc.w, 1, 8);
@@ -362,7 +364,7 @@ __device__ __forceinline__ void plume_direct_unit(const float* __restrict__ C, f
             if (!zb_lane) zb = eb;
             if (!zt_lane) zt = et;
             const float4 v = ftcs4(cc, cw, ce, cs, cn, zb, zt, mr, k, w0s);
-            if (act && vd) store_void(Cn + idx, v, vd);
+            if (act && vd) store_void(Cn + off, v, vd);
         }
         cw = cc;
         cc = ce;
@@ -907,6 +909,7 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     const PlumeTab tab = make_plume_tab(c);
     const int nx = p->nx, ny = p->ny, nz = p->nz;
     const int mz = plume_mask_pitch(nz);
+    BD_REQUIRE((long long)nx * ny * mz < (1LL << 31), "plume: grid %dx%dx%d exceeds 2^31 mask bytes", nx, ny, nz);
     const int* zl = full_first ? nullptr : zlimit;
     k_plume_mask<<<dim3((ny + PM_TY - 1) / PM_TY, nx), dim3(PM_TZ, PM_TY), 0, st>>>(nx, ny, nz, mz, F, mask, zl);
     BD_CHECK_LAUNCH("k_plume_mask");
@@ -1164,6 +1167,7 @@ int plume_batch_launch(int n, const PlumeInstHost* insts, const int* order, cons
     const BdPlumeParams* p = insts[0].params;
     const int nx = p->nx, ny = p->ny, nz = p->nz;
     const int mz = plume_mask_pitch(nz);
+    BD_REQUIRE((long long)nx * ny * mz < (1LL << 31), "plume batch: grid exceeds 2^31 mask bytes");
     const int xc = tune_value(BD_TUNE_PLUME_XC);
     const int n_yt = (ny + PD_BY - 1) / PD_BY, n_xch = (nx + xc - 1) / xc;
     const size_t zoff = plume_zlist_offset(nx, ny, nz);
