@@ -174,9 +174,10 @@ def _epoch_ms(eng, n_epochs: int, laser: bool) -> float:
 def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=None) -> dict:
     """Pick launch shapes by timing them on a throwaway engine of the real workload: `inst` is a
     campaign instance dict or a callable returning an engine with a `laser_power` attribute.
-    MC CTAs per SM (photons per thread) are timed by the MC stage of laser-on epochs; x-planes per
-    CTA of the fused substep kernel by the whole epoch with the laser off (the void domain does not
-    change between trials). The plume kernel and the direct kernel's x-planes per CTA are searched
+    MC CTAs per SM (photons per thread) are timed by whole laser-on epochs; x-planes per CTA of the
+    fused substep kernel by whole epochs with the laser off (the void domain does not change between
+    trials): the plume stage runs beside MC and the substeps, so a shape that slows its own stage
+    but leaves the plume more room can win. The plume kernel and the direct kernel's x-planes per CTA are searched
     together, also by laser-off epochs; the resident kernel has no x-planes knob and the compact
     kernel chooses its x-planes per stage on the device. Sets
     the winning values process-wide (bd_tune_set) and returns the choices with every trial's time
@@ -184,7 +185,7 @@ def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=
     from . import _lib
     cand = dict(candidates or {})
     cand.setdefault(_lib.TUNE_MC_BLOCKS_PER_SM, [2, 4, 6, 8])
-    cand.setdefault(_lib.TUNE_STENCIL_XC, [4, 8, 16])
+    cand.setdefault(_lib.TUNE_STENCIL_XC, [1, 2, 4, 8, 16])
     cand.setdefault(_lib.TUNE_PLUME_KERNEL, [_lib.PLUME_KERNEL_DIRECT, _lib.PLUME_KERNEL_COMPACT,
                                              _lib.PLUME_KERNEL_RESIDENT])
     cand.setdefault(_lib.TUNE_PLUME_XC, [2, 3, 4, 6])
@@ -198,8 +199,8 @@ def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=
         for knob, v in settings:
             _lib.call("bd_tune_set", int(knob), int(v))
         _stage_ms(eng, 1, laser=mc)          # re-capture the stage graphs for the new shape
-        return (float(_stage_ms(eng, epochs_per_trial, laser=True)[0]) if mc
-                else _epoch_ms(eng, epochs_per_trial, laser=False))
+        # whole epochs: the stages run beside each other, so a stage's own time is not what matters
+        return _epoch_ms(eng, epochs_per_trial, laser=mc)
 
     for knob in (_lib.TUNE_MC_BLOCKS_PER_SM, _lib.TUNE_STENCIL_XC):
         trials = []
