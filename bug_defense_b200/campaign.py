@@ -184,7 +184,7 @@ def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=
     (ms per epoch)."""
     from . import _lib
     cand = dict(candidates or {})
-    cand.setdefault(_lib.TUNE_MC_BLOCKS_PER_SM, [2, 4, 6, 8])
+    cand.setdefault(_lib.TUNE_MC_BLOCKS_PER_SM, [1, 2, 3, 4, 6, 8])
     cand.setdefault(_lib.TUNE_STENCIL_XC, [1, 2, 4, 8, 16])
     cand.setdefault(_lib.TUNE_PLUME_KERNEL, [_lib.PLUME_KERNEL_DIRECT, _lib.PLUME_KERNEL_COMPACT,
                                              _lib.PLUME_KERNEL_RESIDENT])
@@ -202,10 +202,10 @@ def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=
         # whole epochs: the stages run beside each other, so a stage's own time is not what matters
         return _epoch_ms(eng, epochs_per_trial, laser=mc)
 
-    for knob in (_lib.TUNE_MC_BLOCKS_PER_SM, _lib.TUNE_STENCIL_XC):
+    def single(knob, mc):
         trials = []
         for v in cand[knob]:
-            t = trial([(knob, v)], mc=knob == _lib.TUNE_MC_BLOCKS_PER_SM)
+            t = trial([(knob, v)], mc=mc)
             trials.append((int(v), t))
             if log:
                 log(f"autotune {names[knob]}={v}: {t:.3f} ms/epoch")
@@ -213,16 +213,24 @@ def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=
         _lib.call("bd_tune_set", int(knob), int(best))
         out[names[knob]] = best
         out["trials"][names[knob]] = trials
-    # plume kernel x x-planes per CTA (only the one-launch-per-step grid kernel takes the knob)
-    trials = []
-    for kern in cand[_lib.TUNE_PLUME_KERNEL]:
-        xcs = cand[_lib.TUNE_PLUME_XC] if kern == _lib.PLUME_KERNEL_DIRECT else [None]
-        for xc in xcs:
+
+    # laser-off trials first, on the state the run starts from (they leave the void domain as it is);
+    # the MC trials, whose laser epochs deepen the crater, come last
+    single(_lib.TUNE_STENCIL_XC, False)
+    # plume kernel x x-planes per CTA (only the one-launch-per-step grid kernel takes the knob); the
+    # candidates differ by a few per cent, so each is timed twice (forward, then reversed order) and
+    # keeps its better time
+    combos = [(int(kern), xc) for kern in cand[_lib.TUNE_PLUME_KERNEL]
+              for xc in (cand[_lib.TUNE_PLUME_XC] if kern == _lib.PLUME_KERNEL_DIRECT else [None])]
+    best_t = {}
+    for order in (combos, combos[::-1]):
+        for kern, xc in order:
             sets = [(_lib.TUNE_PLUME_KERNEL, kern)] + ([] if xc is None else [(_lib.TUNE_PLUME_XC, xc)])
             t = trial(sets)
-            trials.append((int(kern), xc, t))
+            best_t[(kern, xc)] = min(t, best_t.get((kern, xc), float("inf")))
             if log:
                 log(f"autotune plume_kernel={kern} plume_xc={xc}: {t:.3f} ms/epoch")
+    trials = [(kern, xc, best_t[(kern, xc)]) for kern, xc in combos]
     kern, xc, _ = min(trials, key=lambda t: t[2])
     _lib.call("bd_tune_set", _lib.TUNE_PLUME_KERNEL, kern)
     if xc is not None:
@@ -234,6 +242,7 @@ def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=
     out["plume_kernel"] = kern
     out["plume_xc"] = int(xc)
     out["trials"]["plume"] = [[k, x, t] for k, x, t in trials]
+    single(_lib.TUNE_MC_BLOCKS_PER_SM, True)
     del eng
     return out
 
