@@ -164,6 +164,7 @@ TUNE_MC_BLOCKS_PER_SM = 0
 TUNE_STENCIL_XC = 1
 TUNE_PLUME_XC = 2
 TUNE_PLUME_KERNEL = 3
+TUNE_STENCIL_CAP = 4
 PLUME_KERNEL_DIRECT = 4
 PLUME_KERNEL_RESIDENT = 5
 PLUME_KERNEL_COMPACT = 6

@@ -189,8 +189,10 @@ def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=
     cand.setdefault(_lib.TUNE_PLUME_KERNEL, [_lib.PLUME_KERNEL_DIRECT, _lib.PLUME_KERNEL_COMPACT,
                                              _lib.PLUME_KERNEL_RESIDENT])
     cand.setdefault(_lib.TUNE_PLUME_XC, [2, 3, 4, 6])
+    cand.setdefault(_lib.TUNE_STENCIL_CAP, [0, 1, 2])
     names = {_lib.TUNE_MC_BLOCKS_PER_SM: "mc_ctas_per_sm", _lib.TUNE_STENCIL_XC: "stencil_xc",
-             _lib.TUNE_PLUME_XC: "plume_xc", _lib.TUNE_PLUME_KERNEL: "plume_kernel"}
+             _lib.TUNE_PLUME_XC: "plume_xc", _lib.TUNE_PLUME_KERNEL: "plume_kernel",
+             _lib.TUNE_STENCIL_CAP: "stencil_cap"}
     eng = inst() if callable(inst) else make_engine(inst, device=device)
     eng.step_epochs(3)                       # warm-up: graphs, caches, a first crater
     out = {"trials": {}}
@@ -217,6 +219,7 @@ def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=
     # laser-off trials first, on the state the run starts from (they leave the void domain as it is);
     # the MC trials, whose laser epochs deepen the crater, come last
     single(_lib.TUNE_STENCIL_XC, False)
+    single(_lib.TUNE_STENCIL_CAP, False)
     # plume kernel x x-planes per CTA (only the one-launch-per-step grid kernel takes the knob); the
     # candidates differ by a few per cent, so each is timed twice (forward, then reversed order) and
     # keeps its better time

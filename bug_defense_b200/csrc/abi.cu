@@ -32,7 +32,7 @@ int cuda_status(cudaError_t e, const char* what) {
     return BD_ERR_CUDA;
 }
 
-static std::atomic<int> g_tune[BD_TUNE_COUNT] = {{0}, {8}, {4}, {BD_PLUME_KERNEL_DIRECT}};
+static std::atomic<int> g_tune[BD_TUNE_COUNT] = {{0}, {8}, {4}, {BD_PLUME_KERNEL_DIRECT}, {0}};
 static std::atomic<int> g_tune_gen{0};
 
 int tune_value(int knob) { return g_tune[knob].load(std::memory_order_relaxed); }
@@ -46,6 +46,8 @@ extern "C" int bd_tune_set(int knob, int value) {
     BD_REQUIRE(knob >= 0 && knob < BD_TUNE_COUNT, "bd_tune_set: unknown knob %d", knob);
     if (knob == BD_TUNE_MC_BLOCKS_PER_SM)
         BD_REQUIRE(value >= 0 && value <= 16, "bd_tune_set: MC CTAs per SM must be 0..16, got %d", value);
+    else if (knob == BD_TUNE_STENCIL_CAP)
+        BD_REQUIRE(value >= 0 && value <= 16, "bd_tune_set: substep CTAs per SM cap must be 0..16, got %d", value);
     else if (knob == BD_TUNE_PLUME_KERNEL)
         BD_REQUIRE(value == BD_PLUME_KERNEL_DIRECT || value == BD_PLUME_KERNEL_RESIDENT ||
                        value == BD_PLUME_KERNEL_COMPACT,

@@ -311,6 +311,25 @@ static Geo make_geo(int nx, int ny, int nz, float dx, float dy, float dz, float 
     return g;
 }
 
+// Unused dynamic shared memory that lets at most `cap` substep CTAs share an SM (0: no cap). The
+// plume stage runs beside the substeps; capping them leaves the plume's CTAs room on every SM (16 KB
+// of shared memory per SM stay free for them). The kernel's limit is raised once per instantiation.
+static size_t substep_pad_bytes(int cap, const void* kernel) {
+    if (cap <= 0) return 0;
+    int dev = 0, per_sm = 0, per_block = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return 0;
+    const long long reserve = 1024;                  // per-CTA shared memory the system keeps
+    long long pad = ((long long)per_sm - 16384) / cap - (long long)fa.sharedSizeBytes - reserve;
+    pad = std::max(0LL, std::min(pad, (long long)per_block - (long long)fa.sharedSizeBytes));
+    if (pad > 48 * 1024 && fa.maxDynamicSharedSizeBytes < pad)
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pad);
+    return (size_t)pad;
+}
+
 template <int MODE, int BC, bool ARR, bool CHAR>
 static void launch_substeps(const Geo& g, const AblConst& c, float* Ta, float* Tb, int n, const float* src,
                             const float* K, const float* R, const uint8_t* F, float* H, float* Om, float* Chi,
@@ -325,10 +344,11 @@ static void launch_substeps(const Geo& g, const AblConst& c, float* Ta, float* T
     if (tma) {
         const int xc = tune_value(BD_TUNE_STENCIL_XC);
         const dim3 grid((g.nz + ST_BZ - 1) / ST_BZ, (g.ny + ST_BY - 1) / ST_BY, (g.nx + xc - 1) / xc);
+        const size_t pad = substep_pad_bytes(tune_value(BD_TUNE_STENCIL_CAP), (const void*)k_substep_tma<MODE, BC, ARR, CHAR>);
         for (int s = 0; s < n; ++s) {
             float* out = (s & 1) ? Ta : Tb;
-            k_substep_tma<MODE, BC, ARR, CHAR><<<grid, dim3(TZ, TY), 0, st>>>((s & 1) ? mb : ma, mk, g, c, out, src,
-                                                                             R, F, H, Om, Chi, xc, err);
+            k_substep_tma<MODE, BC, ARR, CHAR><<<grid, dim3(TZ, TY), pad, st>>>((s & 1) ? mb : ma, mk, g, c, out, src,
+                                                                               R, F, H, Om, Chi, xc, err);
         }
         return;
     }

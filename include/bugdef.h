@@ -395,7 +395,9 @@ BD_API int bd_engine_record(BdEngine* e, const BdRecordSpec* spec, void* slot, v
                                         used), so no empty CTA is dispatched and no partial second wave
                                         runs. Same results as BD_PLUME_KERNEL_DIRECT; nz % 4 != 0 falls
                                         back to it                                                      */
-#define BD_TUNE_COUNT             4
+#define BD_TUNE_STENCIL_CAP       4  /* at most this many substep CTAs per SM (0 = no cap, default): the
+                                        plume stage runs beside the substeps and keeps the rest         */
+#define BD_TUNE_COUNT             5
 BD_API int bd_tune_set(int knob, int value);
 BD_API int bd_tune_get(int knob, int* value);
 

@@ -22,7 +22,7 @@ def _knob(k, v=None):
 def restore_knobs(gpu):
     from bug_defense_b200 import _lib
     keep = {k: _knob(k) for k in (_lib.TUNE_MC_BLOCKS_PER_SM, _lib.TUNE_STENCIL_XC, _lib.TUNE_PLUME_XC,
-                                  _lib.TUNE_PLUME_KERNEL)}
+                                  _lib.TUNE_PLUME_KERNEL, _lib.TUNE_STENCIL_CAP)}
     yield
     for k, v in keep.items():
         _knob(k, v)
@@ -37,6 +37,9 @@ def test_knob_validation(gpu, restore_knobs):
     for bad in (0, 3, 7):
         with pytest.raises(ValueError):
             _knob(_lib.TUNE_PLUME_KERNEL, bad)
+    for bad in (-1, 17):
+        with pytest.raises(ValueError):
+            _knob(_lib.TUNE_STENCIL_CAP, bad)
     with pytest.raises(ValueError):
         _knob(7, 1)
 
@@ -48,11 +51,12 @@ def test_launch_shapes_leave_results_bit_identical(gpu, restore_knobs):
     T0 = 25 + 50 * rng.random(n); Q = rng.random(n) * 1e-3
     K = 1e-4 + 5e-4 * rng.random(n); R = 2e-3 + 2e-3 * rng.random(n)
     outs = []
-    for xc in (4, 8, 16):
+    for xc, cap in ((4, 0), (8, 1), (16, 2), (1, 0)):
         _knob(_lib.TUNE_STENCIL_XC, xc)
+        _knob(_lib.TUNE_STENCIL_CAP, cap)
         outs.append(thermal.run_thermal3d_substeps_gpu(T0, Q, K, R, *n, 0.015, 0.015, 0.015, 5e-5, 9, h_eff=2e-5,
                                                        t_ambient=25.0, is_active=1))
-    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+    assert all(np.array_equal(outs[0], o) for o in outs[1:])
     cube = {k: np.full((16, 16, 20), v) for k, v in (("mu_a", 2.0), ("mu_s", 15.0), ("g", 0.85), ("n", 1.4))}
     kw = dict(n_photons=60_000, base_seed=77, Lx=0.24, Ly=0.24, Lz=0.3, Nx=16, Ny=16, Nz=20, custom_3d_props=cube,
               spot_dia=0.1)
@@ -177,8 +181,10 @@ def test_autotune_sets_the_fastest_candidates(gpu, restore_knobs):
     from bug_defense_b200 import _lib, campaign
     res = campaign.autotune(_small(4), epochs_per_trial=2,
                             candidates={_lib.TUNE_MC_BLOCKS_PER_SM: [2, 4], _lib.TUNE_STENCIL_XC: [4, 8],
-                                        _lib.TUNE_PLUME_KERNEL: [4, 6, 5], _lib.TUNE_PLUME_XC: [2, 4]})
-    for name, knob in (("mc_ctas_per_sm", _lib.TUNE_MC_BLOCKS_PER_SM), ("stencil_xc", _lib.TUNE_STENCIL_XC)):
+                                        _lib.TUNE_PLUME_KERNEL: [4, 6, 5], _lib.TUNE_PLUME_XC: [2, 4],
+                                        _lib.TUNE_STENCIL_CAP: [0, 2]})
+    for name, knob in (("mc_ctas_per_sm", _lib.TUNE_MC_BLOCKS_PER_SM), ("stencil_xc", _lib.TUNE_STENCIL_XC),
+                       ("stencil_cap", _lib.TUNE_STENCIL_CAP)):
         trials = res["trials"][name]
         assert [v for v, _ in trials] == sorted(v for v, _ in trials) and all(t > 0 for _, t in trials)
         assert res[name] == min(trials, key=lambda t: t[1])[0] == _knob(knob)
