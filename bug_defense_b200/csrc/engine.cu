@@ -276,6 +276,10 @@ extern "C" int bd_engine_set_time(BdEngine* e, double t, int64_t epoch, void* st
 extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void* stream) {
     BD_REQUIRE(e != nullptr, "bd_engine_step_epoch: NULL engine");
     BD_REQUIRE(power >= 0.0f, "bd_engine_step_epoch: power must be >= 0");
+    const bool external = (options & BD_EPOCH_EXTERNAL_PLUME) != 0;
+    BD_REQUIRE(!(external && e->ring_on),
+               "bd_engine_step_epoch: BD_EPOCH_EXTERNAL_PLUME epochs are not covered by the stage-timing ring; "
+               "turn timing off first");
     cudaStream_t st = as_stream(stream);
     const BdEngineDesc& d = e->d;
     const long long nv = (long long)d.phase.nx * d.phase.ny * d.phase.nz;
@@ -291,7 +295,6 @@ extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void*
 
     const bool laser = power > 0.0f;
     int rc = BD_OK;
-    const bool external = (options & BD_EPOCH_EXTERNAL_PLUME) != 0;
     const bool plume = d.n_substeps > 0 && d.has_plume_transport && !external;
     const bool conc = plume && e->side && !(options & BD_EPOCH_SERIAL_PLUME) && !plume_resident_active(&d.plume);
     auto plume_stage = [&](cudaStream_t on) -> int {

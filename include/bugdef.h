@@ -292,7 +292,7 @@ typedef struct BdEpochDiag {
                                       instead of beside MC + substeps on the engine's plume stream */
 #define BD_EPOCH_EXTERNAL_PLUME 0x8 /* enqueue the epoch's start, MC and substeps only: the caller runs
                                       the plume stage (bd_plume_batch_run) and then the epoch end
-                                      (bd_engine_epoch_finish)                                      */
+                                      (bd_engine_epoch_finish); rejected while stage timing is on */
 
 typedef struct BdEngine BdEngine;
 /* Replaces CoupledAblationEngine.__init__ device setup (coupled_ablation.py:184-407);
