@@ -311,16 +311,21 @@ def e2e_run(args, geo, dev, K):
     torch.cuda.synchronize()
     st = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    from bug_defense_b200._device import upload_stats
+    up0 = dict(upload_stats)
     e0.record(st)
     h0 = time.perf_counter()
     eng = make_engine(geo, dev, seed_offset=101)
     h1 = time.perf_counter()
     ec = torch.cuda.Event(enable_timing=True)
     ec.record(st)
-    h2d = sum(np.asarray(v).nbytes for v in (geo["optical"]["mu_a"], geo["optical"]["mu_s"], geo["optical"]["g"],
-                                               geo["optical"]["n"], geo["k_grid"], geo["rho_cp_grid"],
-                                               geo["h_lat_grid"], geo["dry_mask"], geo["ablated_mask"]))
-    h2d += sum(np.asarray(geo["dry_state"][k]).nbytes for k in ("mu_a", "mu_s", "g", "n", "k", "rho_cp"))
+    # bytes that crossed host->device (grids that are one z column broadcast over x and y travel as
+    # that column) and the host input the constructor read
+    h2d = upload_stats["bytes"] - up0["bytes"]
+    host_in = sum(np.asarray(v).nbytes for v in (geo["optical"]["mu_a"], geo["optical"]["mu_s"], geo["optical"]["g"],
+                                                 geo["optical"]["n"], geo["k_grid"], geo["rho_cp_grid"],
+                                                 geo["h_lat_grid"], geo["dry_mask"], geo["ablated_mask"]))
+    host_in += sum(np.asarray(geo["dry_state"][k]).nbytes for k in ("mu_a", "mu_s", "g", "n", "k", "rho_cp"))
     n_on = max(1, int(round(LASER_DUTY * K)))
     # the runner's per-epoch recording through the public Recorder: the device record kernel fills
     # a slot (xz slices of T, Q, phase and plume at mid-y, depth, band peaks) that is copied into a
@@ -337,7 +342,10 @@ def e2e_run(args, geo, dev, K):
     ms = e0.elapsed_time(e1)
     return {"value": K / (ms / 1e3), "unit": "epochs/s", "h2d_bytes_per_step": int(h2d / K),
             "d2h_bytes_per_step": int(d2h), "construct_ms": round(e0.elapsed_time(ec), 2),
-            "construct_host_ms": round((h1 - h0) * 1e3, 2),
+            "construct_host_ms": round((h1 - h0) * 1e3, 2), "host_input_bytes": int(host_in),
+            "construct_h2d_bytes": int(h2d),
+            "column_grids": upload_stats["column_grids"] - up0["column_grids"],
+            "full_grids": upload_stats["full_grids"] - up0["full_grids"],
             "epochs_ms": round(ec.elapsed_time(e1), 2), "note": "engine construction from host arrays + per-epoch diagnostics "
                                                      "and xz recording slices, amortised over the timed epochs"}
 

@@ -1,6 +1,10 @@
 """Device selection and host<->device helpers (torch is only the memory/stream plumbing)."""
 from __future__ import annotations
 
+import os
+import threading
+from concurrent.futures import ThreadPoolExecutor
+
 import numpy as np
 import torch
 
@@ -37,21 +41,98 @@ def require_device(device=None) -> torch.device:
     return dev
 
 
+# Grids at least this large (elements) are checked for the per-slice column form before upload.
+_COLUMN_MIN = 1 << 16
+_UINT = {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}
+_NP = {torch.float32: np.float32, torch.float64: np.float64, torch.uint8: np.uint8, torch.bool: np.bool_}
+_WORKERS = max(1, min(16, os.cpu_count() or 1))
+_pool = None
+_pool_lock = threading.Lock()
+
+# Host->device bytes copied by to_dev (all callers): the end-to-end benchmark reports them.
+upload_stats = {"bytes": 0, "column_grids": 0, "full_grids": 0}
+
+
+def _executor() -> ThreadPoolExecutor:
+    global _pool
+    with _pool_lock:
+        if _pool is None:
+            _pool = ThreadPoolExecutor(max_workers=_WORKERS, thread_name_prefix="bd-column-check")
+        return _pool
+
+
+def slice_column(arr: np.ndarray):
+    """The z column c when a C-order (nx, ny, nz) grid holds c at every (x, y), else None.
+
+    Layered stacks are built that way: the production runner's geometry and the configs' stacks
+    give every property per z slice and broadcast it over x and y
+    (run_highres_knowledge_suite.py:126-185). Such a grid is uploaded as its column and expanded
+    on the device, which moves nz values over PCIe instead of nx*ny*nz. The comparison is bitwise
+    (the grid viewed as unsigned integers), so -0.0, NaN payloads and every other bit pattern are
+    kept exactly; it runs in ~1 MB chunks on a thread pool (numpy releases the GIL in the
+    comparison loops) and stops at the first chunk that differs, after three sample columns have
+    been compared first."""
+    if arr.ndim != 3 or arr.size < _COLUMN_MIN or arr.shape[0] * arr.shape[1] < 2:
+        return None
+    if arr.dtype.kind not in "biuf" or arr.dtype.itemsize not in _UINT:
+        return None
+    nx, ny, nz = arr.shape
+    if arr.strides[0] == 0 and arr.strides[1] == 0:  # a broadcast view: the column form already
+        return np.ascontiguousarray(arr[0, 0])
+    if not arr.flags.c_contiguous:
+        return None
+    rows = arr.reshape(nx * ny, nz).view(_UINT[arr.dtype.itemsize])
+    col = rows[0]
+    n = nx * ny
+    for r in (n - 1, (nx // 2) * ny + ny // 2, 1):
+        if not np.array_equal(rows[r], col):
+            return None
+    differs = threading.Event()
+    step = max(1, (1 << 20) // (nz * arr.dtype.itemsize))
+
+    def check(lo, hi):
+        for i in range(lo, hi, step):
+            if differs.is_set():
+                return False
+            if not (rows[i:min(i + step, hi)] == col).all():
+                differs.set()
+                return False
+        return True
+
+    pool = _executor()
+    parts = max(1, min(_WORKERS, n // step))
+    bounds = [n * i // parts for i in range(parts + 1)]
+    if not all(list(pool.map(check, bounds[:-1], bounds[1:]))):
+        return None
+    return np.ascontiguousarray(arr[0, 0])
+
+
 def to_dev(a, dev, dtype=torch.float32) -> torch.Tensor:
-    """Contiguous device copy of a numpy array / scalar / tensor."""
+    """Contiguous device copy of a numpy array / scalar / tensor.
+
+    A numpy grid that is one z column broadcast over x and y (slice_column) crosses PCIe as that
+    column and is expanded on the device; the result has the same bits either way."""
     if isinstance(a, torch.Tensor):
         return a.to(device=dev, dtype=dtype).contiguous()
-    arr = np.ascontiguousarray(a)
-    if dtype == torch.float32 and arr.dtype == np.float64:
-        # upload as is and round on the device (the same IEEE round-to-nearest as numpy's astype)
-        return torch.from_numpy(arr).to(dev).to(torch.float32)
-    if dtype == torch.uint8:
-        arr = arr.astype(np.uint8, copy=False)
-    elif dtype == torch.float32:
-        arr = arr.astype(np.float32, copy=False)
-    elif dtype == torch.float64:
-        arr = arr.astype(np.float64, copy=False)
-    return torch.from_numpy(arr).to(dev)
+    arr = np.asarray(a)
+    # float64 -> float32: upload as is and round on the device (the same IEEE round-to-nearest as
+    # numpy's astype); other conversions happen on the host
+    round_on_device = dtype == torch.float32 and arr.dtype == np.float64
+    if not round_on_device and dtype in _NP:
+        arr = arr.astype(_NP[dtype], copy=False)
+    col = slice_column(arr)
+    if col is not None:
+        t = torch.from_numpy(col).to(dev)
+        upload_stats["bytes"] += col.nbytes
+        upload_stats["column_grids"] += 1
+        if round_on_device:
+            t = t.to(torch.float32)
+        return t.expand(arr.shape).contiguous()
+    arr = np.ascontiguousarray(arr)
+    t = torch.from_numpy(arr).to(dev)
+    upload_stats["bytes"] += arr.nbytes
+    upload_stats["full_grids"] += 1
+    return t.to(torch.float32) if round_on_device else t
 
 
 def full_grid(value, shape, dev, dtype=torch.float32) -> torch.Tensor:

@@ -93,12 +93,12 @@ class CoupledAblationEngine:
         def h64(a):
             if isinstance(a, torch.Tensor):
                 return a.to(device=d, dtype=torch.float64).clone()
-            return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(d)
+            return to_dev(a, d, torch.float64)
 
         def hbool(a):
             if isinstance(a, torch.Tensor):
                 return a.to(device=d).bool()
-            return torch.from_numpy(np.ascontiguousarray(a, dtype=np.bool_)).to(d)
+            return to_dev(a, d, torch.bool)
 
         optical = {key: h64(optical_props[key]) for key in ('mu_a', 'mu_s', 'g', 'n')}
         self.Nx, self.Ny, self.Nz = optical['mu_a'].shape

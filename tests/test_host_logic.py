@@ -122,3 +122,38 @@ def test_engine_wait_hooks_run_once_each_and_drop_dead_owners():
     gc.collect()
     eng._run_wait_hooks()
     assert calls == ["a", "b", "a"] and len(eng._wait_hooks) == 1
+
+
+def test_layered_grids_upload_as_columns_with_the_same_bits():
+    """to_dev sends a grid that is one z column broadcast over x and y as that column and expands it
+    on the device; any grid that differs anywhere (one bit, -0.0 against 0.0) is copied whole."""
+    import torch
+    from bug_defense_b200 import _device
+    from bug_defense_b200._device import slice_column, to_dev
+    rng = np.random.default_rng(3)
+    nx, ny, nz = 48, 40, 64
+    col = rng.normal(size=nz)
+    col[5] = np.nan
+    col[7] = -0.0
+    layered = np.broadcast_to(col, (nx, ny, nz)).copy()
+    assert slice_column(layered) is not None
+    assert slice_column(np.broadcast_to(col, (nx, ny, nz))) is not None      # a broadcast view
+    for ix, iy, kz in ((0, 1, 3), (nx - 1, ny - 1, nz - 1), (17, 23, 7), (nx // 2, ny // 2, 0)):
+        other = layered.copy()
+        other[ix, iy, kz] = 0.0 if kz == 7 else np.nextafter(other[ix, iy, kz], np.inf)
+        assert slice_column(other) is None, (ix, iy, kz)
+    assert slice_column(layered[:, :, ::2]) is None                           # not C-contiguous
+    assert slice_column(np.ones((4, 4, 8))) is None                           # below the size floor
+    mask = np.zeros((nx, ny, nz), bool)
+    mask[:, :, 10:20] = True
+    assert np.array_equal(slice_column(mask), mask[0, 0])
+    before = dict(_device.upload_stats)
+    for arr, dt in ((layered, torch.float64), (layered, torch.float32), (mask, torch.bool), (mask, torch.uint8),
+                    (rng.normal(size=(nx, ny, nz)), torch.float64)):
+        t = to_dev(arr, torch.device("cpu"), dt)
+        want = torch.from_numpy(np.ascontiguousarray(arr)).to(dt)
+        assert t.shape == arr.shape and t.dtype == dt and t.is_contiguous()
+        assert torch.equal(t.view(torch.uint8), want.contiguous().view(torch.uint8))
+    assert _device.upload_stats["column_grids"] - before["column_grids"] == 4
+    assert _device.upload_stats["full_grids"] - before["full_grids"] == 1
+    assert _device.upload_stats["bytes"] - before["bytes"] == 2 * nz * 8 + 2 * nz + nx * ny * nz * 8
