@@ -49,8 +49,8 @@ def parse():
     ap.add_argument("--no-denoiser", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-full-run", action="store_true", help="skip the device-timed 1000-epoch schedule")
-    ap.add_argument("--plume-kernel", type=int, default=None, choices=[4, 5, 6],
-                    help="plume kernel to use (4 direct, 5 resident, 6 direct over a compact unit list) instead of "
+    ap.add_argument("--plume-kernel", type=int, default=None, choices=[4, 6],
+                    help="plume kernel to use (4 direct, 6 direct over a compact unit list) instead of "
                          "the autotuner's choice")
     ap.add_argument("--batch-plume", action="store_true",
                     help="campaign: run the instances' plume stages as one batched stage (one launch per step)")
@@ -403,8 +403,7 @@ def ours_main(args):
     from bug_defense_b200 import _lib
     kv = ctypes.c_int(0)
     _lib.call("bd_tune_get", _lib.TUNE_PLUME_KERNEL, ctypes.byref(kv))
-    plume_kernel = {4: "k_plume_direct_z", 5: "k_plume_resident",
-                    6: "k_plume_direct_c"}.get(kv.value, "k_plume_step")
+    plume_kernel = {4: "k_plume_direct_z", 6: "k_plume_direct_c"}.get(kv.value, "k_plume_step")
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():

@@ -166,7 +166,6 @@ TUNE_PLUME_XC = 2
 TUNE_PLUME_KERNEL = 3
 TUNE_STENCIL_CAP = 4
 PLUME_KERNEL_DIRECT = 4
-PLUME_KERNEL_RESIDENT = 5
 PLUME_KERNEL_COMPACT = 6
 
 CONV_FWD_RELU = 0

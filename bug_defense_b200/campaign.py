@@ -178,16 +178,15 @@ def autotune(inst, epochs_per_trial: int = 6, candidates=None, device=None, log=
     fused substep kernel by whole epochs with the laser off (the void domain does not change between
     trials): the plume stage runs beside MC and the substeps, so a shape that slows its own stage
     but leaves the plume more room can win. The plume kernel and the direct kernel's x-planes per CTA are searched
-    together, also by laser-off epochs; the resident kernel has no x-planes knob and the compact
-    kernel chooses its x-planes per stage on the device. Sets
+    together, also by laser-off epochs; the compact kernel chooses its x-planes per stage on the
+    device. Sets
     the winning values process-wide (bd_tune_set) and returns the choices with every trial's time
     (ms per epoch)."""
     from . import _lib
     cand = dict(candidates or {})
     cand.setdefault(_lib.TUNE_MC_BLOCKS_PER_SM, [1, 2, 3, 4, 6, 8])
     cand.setdefault(_lib.TUNE_STENCIL_XC, [1, 2, 4, 8, 16])
-    cand.setdefault(_lib.TUNE_PLUME_KERNEL, [_lib.PLUME_KERNEL_DIRECT, _lib.PLUME_KERNEL_COMPACT,
-                                             _lib.PLUME_KERNEL_RESIDENT])
+    cand.setdefault(_lib.TUNE_PLUME_KERNEL, [_lib.PLUME_KERNEL_DIRECT, _lib.PLUME_KERNEL_COMPACT])
     cand.setdefault(_lib.TUNE_PLUME_XC, [2, 3, 4, 6])
     cand.setdefault(_lib.TUNE_STENCIL_CAP, [0, 1, 2])
     names = {_lib.TUNE_MC_BLOCKS_PER_SM: "mc_ctas_per_sm", _lib.TUNE_STENCIL_XC: "stencil_xc",
@@ -255,10 +254,8 @@ class Campaign:
     host synchronisation between them (diagnostics are read every `sync_every` epochs). The laser
     of instance i is on for its first epochs_on epochs.
 
-    With the resident plume kernel (BD_PLUME_KERNEL_RESIDENT) each instance's plume stage occupies every SM, so
-    the instances share one CUDA stream: two resident stages on concurrent streams could each hold
-    part of the GPU while waiting for the rest. Otherwise every instance gets its own stream and
-    runs its own plume stage beside its own MC and substeps. With `batch_plume` the instances' plume
+    Every instance gets its own stream and runs its own plume stage beside its own MC and
+    substeps. With `batch_plume` the instances' plume
     stages instead run as one batched stage (bd_plume_batch_run: one launch per FTCS step over the
     live units of every instance still stepping) on a stream of its own, beside the instances' MC and
     substeps, and each instance's epoch end waits for it. Same results; measured slower on the
@@ -271,22 +268,16 @@ class Campaign:
         self.instances = list(instances)
         self.engines = []
         self.streams = []
-        kv = ctypes.c_int(0)
-        _lib.call("bd_tune_get", _lib.TUNE_PLUME_KERNEL, ctypes.byref(kv))
-        self.shared_stream = kv.value == _lib.PLUME_KERNEL_RESIDENT
         t0 = time.perf_counter()
         for inst in self.instances:
             eng = make_engine(inst, device=device, use_graphs=use_graphs)
             self.engines.append(eng)
-            if self.shared_stream and self.streams:
-                self.streams.append(self.streams[0])
-            else:
-                self.streams.append(torch.cuda.Stream(device=eng.dev))
+            self.streams.append(torch.cuda.Stream(device=eng.dev))
             if log:
                 log(f"instance {inst['index']}: {inst['wavelength_nm']:.0f} nm, {inst['power']:.0f} W, "
                     f"pulse {inst['pulse_ms']:.0f} ms")
         self.batch = None
-        if batch_plume and not self.shared_stream and len(self.engines) <= 32 and use_graphs:
+        if batch_plume and len(self.engines) <= 32 and use_graphs:
             n = len(self.engines)
             arr = (ctypes.c_void_p * n)(*[e._handle for e in self.engines])
             h = ctypes.c_void_p()

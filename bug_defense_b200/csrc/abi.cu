@@ -49,10 +49,9 @@ extern "C" int bd_tune_set(int knob, int value) {
     else if (knob == BD_TUNE_STENCIL_CAP)
         BD_REQUIRE(value >= 0 && value <= 16, "bd_tune_set: substep CTAs per SM cap must be 0..16, got %d", value);
     else if (knob == BD_TUNE_PLUME_KERNEL)
-        BD_REQUIRE(value == BD_PLUME_KERNEL_DIRECT || value == BD_PLUME_KERNEL_RESIDENT ||
-                       value == BD_PLUME_KERNEL_COMPACT,
-                   "bd_tune_set: plume kernel must be %d (direct), %d (resident) or %d (compact), got %d",
-                   BD_PLUME_KERNEL_DIRECT, BD_PLUME_KERNEL_RESIDENT, BD_PLUME_KERNEL_COMPACT, value);
+        BD_REQUIRE(value == BD_PLUME_KERNEL_DIRECT || value == BD_PLUME_KERNEL_COMPACT,
+                   "bd_tune_set: plume kernel must be %d (direct) or %d (compact), got %d", BD_PLUME_KERNEL_DIRECT,
+                   BD_PLUME_KERNEL_COMPACT, value);
     else
         BD_REQUIRE(value >= 1 && value <= 64, "bd_tune_set: x-planes per CTA must be 1..64, got %d", value);
     if (g_tune[knob].exchange(value) != value) g_tune_gen.fetch_add(1);

@@ -47,13 +47,8 @@ inline size_t plume_units_bytes(int nx, int ny, int nz) {
     const size_t bands = ((size_t)(nz + 3) / 4 + 7) / 8;
     return ((16 + cols * 8 + cols * bands) * sizeof(unsigned) + 255) / 256 * 256;
 }
-// Then the per-CTA step counters of the resident plume kernel (at most kPlumeMaxTiles CTAs).
-constexpr int kPlumeMaxTiles = 256;
-inline size_t plume_flags_offset(int nx, int ny, int nz) {
-    return plume_units_offset(nx, ny, nz) + plume_units_bytes(nx, ny, nz);
-}
 inline size_t plume_mask_bytes(int nx, int ny, int nz) {
-    return plume_flags_offset(nx, ny, nz) + sizeof(unsigned) * kPlumeMaxTiles;
+    return plume_units_offset(nx, ny, nz) + plume_units_bytes(nx, ny, nz);
 }
 
 // Launch-shape knobs (BD_TUNE_*) and the generation counter bumped by every change.

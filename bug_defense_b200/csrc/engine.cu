@@ -296,12 +296,12 @@ extern "C" int bd_engine_step_epoch(BdEngine* e, float power, int options, void*
     const bool laser = power > 0.0f;
     int rc = BD_OK;
     const bool plume = d.n_substeps > 0 && d.has_plume_transport && !external;
-    const bool conc = plume && e->side && !(options & BD_EPOCH_SERIAL_PLUME) && !plume_resident_active(&d.plume);
+    const bool conc = plume && e->side && !(options & BD_EPOCH_SERIAL_PLUME);
     auto plume_stage = [&](cudaStream_t on) -> int {
         return run_stage(e, e->g_plume, &d.plume, sizeof(d.plume), graphs, on, [&](cudaStream_t s) -> int {
             int in_b = 0;
             int r = plume_launch(&d.plume, d.phase.plume, d.plume_alt, d.n_substeps, d.phase.flags, &in_b, s,
-                                 &e->dyn->void_zlimit, 0, e->plume_mask, &e->dyn->err);
+                                 &e->dyn->void_zlimit, 0, e->plume_mask);
             if (r) return r;
             if (in_b)
                 BD_CUDA(cudaMemcpyAsync(d.phase.plume, d.plume_alt, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));

@@ -57,7 +57,7 @@ int phase_launch(const PhaseArgs& a, int mode, cudaStream_t st);
 int ablation_launch(const BdAblationParams* p, float* Ta, float* Tb, int n, float* H, float* Om, float* Chi,
                     const uint8_t* F, const float* src, const float* K, const float* R, cudaStream_t st, int* err);
 int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
-                 cudaStream_t st, const int* zlimit, int full_first, uint8_t* mask, int* err);
+                 cudaStream_t st, const int* zlimit, int full_first, uint8_t* mask);
 int plume_policy_steps(const BdPlumeParams* p, int* n_steps, float* dt_step, float* decay_step);
 // One instance of a batched plume stage (several engines' plume stages in one launch per step).
 struct PlumeTab;
@@ -80,9 +80,6 @@ size_t plume_batch_units_words(int n, int nx, int ny, int nz);
 int plume_batch_prepare(int n, const PlumeInstHost* insts, void* dev, int* order, long long* max_steps);
 int plume_batch_launch(int n, const PlumeInstHost* insts, const int* order, const void* dev, long long max_steps,
                        unsigned* units, cudaStream_t st);
-// true when plume stages of this grid run as one resident launch (its CTAs then occupy every SM for
-// the stage, so the engine runs the stage in line rather than beside MC and the substeps)
-bool plume_resident_active(const BdPlumeParams* p);
 // Per-epoch xz recording (record.cu): inputs of one launch.
 struct RecordArgs {
     int nx, ny, nz, y, k_surface, gap_k0, gap_k1;

@@ -3,9 +3,6 @@
 // centre), Dirichlet 0 on the outer walls, clamped at 0, optional first-order decay.
 //
 // Kernels (all evaluate the same per-voxel expression, ftcs1 / ftcs4, so they are bit-identical):
-//   k_plume_resident  (BD_PLUME_KERNEL_RESIDENT): one persistent CTA per column tile of at most
-//                     15 x 20 keeps its tile of the field in shared memory for every step of a stage
-//                     and swaps a one-voxel halo with its four neighbours through L2 per step
 //   k_plume_direct_z  default (BD_PLUME_KERNEL_DIRECT): one launch per step, a CTA per 32 (z) x 16 (y)
 //                     tile column marching x planes over the column's live z groups
 //   k_plume_direct_c  (BD_PLUME_KERNEL_COMPACT): the same per-unit code, one wave of CTAs looping
@@ -117,8 +114,8 @@ __device__ __forceinline__ float ftcs1(float c0, float w, float e, float s, floa
 // Four consecutive z voxels (one float4 and their four mask bytes); zb / zt: the voxels below and
 // above the group. Pairs of voxels go through the packed FP32x2 operations of sm_100 (each lane
 // rounded as the scalar operation), which halves the arithmetic instructions.
-// w0eff: the table of effective centre weights, wherever the caller keeps it (shared memory in the
-// resident kernel, whose lanes index it divergently).
+// w0eff: the table of effective centre weights, wherever the caller keeps it (shared memory in
+// every step kernel).
 __device__ __forceinline__ float4 ftcs4(float4 c, float4 w, float4 e, float4 s, float4 n, float zb, float zt,
                                         unsigned m, const PlumeTab& k, const float* w0eff) {
     const float2 wx = make_float2(k.wx, k.wx), wy = make_float2(k.wy, k.wy);
@@ -555,292 +552,6 @@ __global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_c(const float* __
     }
 }
 
-// ---- k_plume_resident: a whole stage in one launch ------------------------------------------
-// The (x, y) columns are cut into tiles_x x tiles_y tiles of at most RS_TX x RS_TY columns, one CTA
-// per tile, all resident at once (cooperative launch, one CTA per SM). A CTA copies its tile of the
-// field, with a one-column ring of its neighbours' columns, into shared memory for z < min(zl, RS_Z)
-// (zl = void z-limit) and keeps it there for every step of the stage. Warp w owns rows
-// [RS_R w, RS_R w + RS_R) of the tile and lane l the 4-voxel z group l, so the z neighbours of a
-// group come from the neighbouring lanes by shuffle and the y neighbours inside a warp's rows from
-// its own registers; only the rows just above and below the warp's block are read from shared
-// memory. A step marches the tile's x planes keeping the x-1 / x float4 of every row in registers;
-// after a CTA barrier (every read of the plane done) the plane's new values are written in place.
-// The new values of the tile's boundary columns are also stored to the global ping-pong buffer of
-// the next state; after the step a release flag tells the four neighbours, each CTA waits (acquire)
-// for its neighbours' flags and copies their boundary columns into its ring. Neighbours are
-// therefore never more than one step apart, and two global buffers suffice: a buffer is rewritten two
-// steps after it was read. Voxels at z >= RS_Z (craters deeper than the shared-memory column) are
-// updated straight from and to the global ping-pong buffers by the same CTA in the same plane pass.
-// The final state of the tile is written to buffer (n_steps & 1). Every wait is bounded in time: on
-// a timeout the CTA raises *err and stops (the stage result is then undefined and the engine
-// reports BD_ERR_TIMEOUT).
-#ifndef BD_PLUME_RS_R
-#define BD_PLUME_RS_R 2
-#endif
-constexpr int RS_TX = 15, RS_TY = 20, RS_Z = 128, RS_R = BD_PLUME_RS_R;
-constexpr int RS_G = RS_Z / 4;                    // float4 groups per shared-memory column (= warp lanes)
-constexpr int RS_WARPS = (RS_TY + RS_R - 1) / RS_R;
-constexpr int RS_THREADS = 32 * RS_WARPS;
-static_assert(RS_G == 32, "a warp's lanes are the z groups of a shared-memory column");
-// shared field: (RS_TX + 2) planes x (RS_TY + 2) rows of columns, plus RS_R + 1 spare columns read
-// (never used) by the last warp when the tile has fewer rows than the warps cover
-constexpr size_t RS_C_BYTES = ((size_t)(RS_TX + 2) * (RS_TY + 2) + RS_R + 1) * RS_Z * sizeof(float);
-constexpr size_t RS_M_BYTES = (size_t)RS_TX * RS_TY * RS_Z;
-constexpr size_t RS_SMEM = RS_C_BYTES + RS_M_BYTES + 64 * sizeof(float) + 16;
-constexpr int RS_BATCH = 8;   // independent L2 loads a thread issues before storing them to shared memory
-constexpr long long RS_TIMEOUT_NS = 500000000LL;  // 0.5 s per wait (a step takes microseconds)
-
-struct ResidentArgs {
-    float* buf0;          // the field at the start of the stage (the state of even steps)
-    float* buf1;          // the other ping-pong buffer (odd steps)
-    const uint8_t* M;     // neighbourhood bytes (pitch mz)
-    const int* zlimit;    // void z-limit on the device, or nullptr for nz
-    unsigned* flags;      // per CTA: steps completed in this launch (zeroed before the launch)
-    int* err;
-    int nx, ny, nz, mz;
-    int tiles_x, tiles_y, n_steps;
-    PlumeTab k;
-};
-
-__device__ __forceinline__ long long global_ns() {
-    long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-__global__ void __launch_bounds__(RS_THREADS, 1) k_plume_resident(const __grid_constant__ ResidentArgs a) {
-    extern __shared__ __align__(16) unsigned char rs_smem[];
-    float4* Cs4 = reinterpret_cast<float4*>(rs_smem);
-    unsigned* Ms4 = reinterpret_cast<unsigned*>(rs_smem + RS_C_BYTES);
-    float* w0s = reinterpret_cast<float*>(rs_smem + RS_C_BYTES + RS_M_BYTES);
-    volatile int* s_fail = reinterpret_cast<volatile int*>(rs_smem + RS_C_BYTES + RS_M_BYTES + 64 * sizeof(float));
-
-    const int nx = a.nx, ny = a.ny, nz = a.nz;
-    const int zl = a.zlimit ? min(max(*a.zlimit, 0), nz) : nz;
-    if (zl == 0) return;  // no void voxel: nothing to advance (uniform over the grid)
-    const int b = blockIdx.x;
-    const int bx = b % a.tiles_x, by = b / a.tiles_x;
-    const int x0 = bx * nx / a.tiles_x, x1 = (bx + 1) * nx / a.tiles_x;
-    const int y0 = by * ny / a.tiles_y, y1 = (by + 1) * ny / a.tiles_y;
-    const int tx = x1 - x0, ty = y1 - y0;
-    const int zs = min(zl, RS_Z);      // voxels of a column held in shared memory
-    const int Gs = (zs + 3) / 4;       // their float4 groups
-    const int Gg = (zl + 3) / 4 - Gs;  // groups per column kept in global memory (zl > RS_Z)
-    const int row = ty + 2;            // ring rows per plane
-    const int PS = row * RS_G;         // float4 stride of a plane
-    const size_t plane = (size_t)ny * nz;
-    const int tid = threadIdx.x, lane = tid & 31, yb = (tid >> 5) * RS_R;
-    auto gidx = [&](int x, int y, int z) { return ((size_t)x * ny + y) * nz + z; };
-
-    // zero the shared field (ring columns outside the grid and z >= zl stay 0), then load the tile
-    // and its ring (corners excluded) at the stage's start state, and the tile's mask bytes
-    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int i = tid; i < (int)(RS_C_BYTES / 16); i += RS_THREADS) Cs4[i] = z4;
-    if (tid < 64) w0s[tid] = a.k.w0eff[tid];
-    if (tid == 0) *s_fail = 0;
-    __syncthreads();
-    for (int i = tid; i < (tx + 2) * row * Gs; i += RS_THREADS) {
-        const int g = i % Gs, col = i / Gs, ly = col % row, lx = col / row;
-        const int x = x0 + lx - 1, y = y0 + ly - 1;
-        const bool corner = (lx == 0 || lx == tx + 1) && (ly == 0 || ly == ty + 1);
-        if (corner || x < 0 || x >= nx || y < 0 || y >= ny) continue;
-        Cs4[col * RS_G + g] = __ldcg(reinterpret_cast<const float4*>(a.buf0 + gidx(x, y, 4 * g)));
-    }
-    for (int i = tid; i < tx * ty * Gs; i += RS_THREADS) {
-        const int g = i % Gs, col = i / Gs, y = col % ty, px = col / ty;
-        const unsigned m =
-            __ldg(reinterpret_cast<const unsigned*>(a.M + ((size_t)(x0 + px) * ny + y0 + y) * a.mz + 4 * g));
-        Ms4[(px * ty + y) * RS_G + g] = m & zkeep_mask(zl, 4 * g);
-    }
-    __syncthreads();
-
-    // this thread: rows yb .. yb + RS_R - 1 (those below ty are real), z group `lane`
-    bool rv[RS_R];
-#pragma unroll
-    for (int r = 0; r < RS_R; ++r) rv[r] = yb + r < ty && lane < Gs;
-    const int base = (yb + 1) * RS_G + lane;           // float4 index of (plane 0, row yb, lane)
-    float4 cw[RS_R], cc[RS_R];
-#pragma unroll
-    for (int r = 0; r < RS_R; ++r) {
-        cw[r] = Cs4[base + r * RS_G];
-        cc[r] = Cs4[base + PS + r * RS_G];
-    }
-    const bool top_from_global = Gg > 0 && lane == RS_G - 1;
-
-    bool failed = false;
-    for (int t = 0; t < a.n_steps; ++t) {
-        const float* gcur = (t & 1) ? a.buf1 : a.buf0;
-        float* gnxt = (t & 1) ? a.buf0 : a.buf1;
-        for (int px = 0; px < tx; ++px) {
-            const int pb = base + (px + 1) * PS;   // this thread's first row on the centre plane
-            const int x = x0 + px;
-            float4 ce[RS_R], v[RS_R];
-            unsigned m[RS_R];
-#pragma unroll
-            for (int r = 0; r < RS_R; ++r) {
-                ce[r] = Cs4[pb + PS + r * RS_G];
-                m[r] = rv[r] ? Ms4[(px * ty + yb + r) * RS_G + lane] : 0u;
-            }
-            const float4 s_edge = Cs4[pb - RS_G];            // row yb - 1 (a ring row for the first block)
-            const float4 n_edge = Cs4[pb + RS_R * RS_G];     // row yb + RS_R (the ring row after the last)
-#pragma unroll
-            for (int r = 0; r < RS_R; ++r) {
-                float zb = __shfl_up_sync(0xffffffffu, cc[r].w, 1);
-                float zt = __shfl_down_sync(0xffffffffu, cc[r].x, 1);
-                if (lane == 0) zb = 0.0f;                    // z = 0 is a wall: never updated
-                if (lane == RS_G - 1) zt = top_from_global ? __ldcg(gcur + gidx(x, y0 + yb + r, RS_Z)) : 0.0f;
-                const float4 s = r == 0 ? s_edge : cc[r - 1];
-                const float4 n = r == RS_R - 1 ? n_edge : cc[r + 1];
-                v[r] = ftcs4(cc[r], cw[r], ce[r], s, n, zb, zt, m[r], a.k, w0s);
-            }
-            // columns deeper than the shared-memory part: from and to the global buffers
-            for (int p = tid; p < ty * Gg; p += RS_THREADS) {
-                const int y = p / Gg, z = 4 * (Gs + p % Gg), yy = y0 + y;
-                const size_t idx = gidx(x, yy, z);
-                const unsigned mg = __ldg(reinterpret_cast<const unsigned*>(a.M + ((size_t)x * ny + yy) * a.mz + z)) &
-                                    zkeep_mask(zl, z);
-                const float4 c = __ldcg(reinterpret_cast<const float4*>(gcur + idx));
-                const float4 w = x > 0 ? __ldcg(reinterpret_cast<const float4*>(gcur + idx - plane)) : z4;
-                const float4 e = x + 1 < nx ? __ldcg(reinterpret_cast<const float4*>(gcur + idx + plane)) : z4;
-                const float4 s = yy > 0 ? __ldcg(reinterpret_cast<const float4*>(gcur + idx - nz)) : z4;
-                const float4 n = yy + 1 < ny ? __ldcg(reinterpret_cast<const float4*>(gcur + idx + nz)) : z4;
-                const float zb = z == RS_Z ? Cs4[(px + 1) * PS + (y + 1) * RS_G + RS_G - 1].w  // smem z = RS_Z - 1
-                                           : __ldcg(gcur + idx - 1);
-                const float zt = z + 4 < nz ? __ldcg(gcur + idx + 4) : 0.0f;
-                const unsigned vd = mg & 0x40404040u;
-                if (vd) store_void(gnxt + idx, ftcs4(c, w, e, s, n, zb, zt, mg, a.k, w0s), vd);
-            }
-            __syncthreads();  // every read of plane px (and of its neighbours' old values) is done
-            const bool xedge = px == 0 || px == tx - 1;
-#pragma unroll
-            for (int r = 0; r < RS_R; ++r) {
-                if (rv[r]) {
-                    Cs4[pb + r * RS_G] = v[r];
-                    if (xedge || yb + r == 0 || yb + r == ty - 1)
-                        *reinterpret_cast<float4*>(gnxt + gidx(x, y0 + yb + r, 4 * lane)) = v[r];
-                }
-                cw[r] = cc[r];
-                cc[r] = ce[r];
-            }
-        }
-        __syncthreads();  // the step's boundary stores of every thread are issued
-        // the barrier orders every thread's boundary stores before thread 0's release (a release at gpu
-        // scope is cumulative over the writes thread 0 has observed through the barrier)
-        if (tid == 0) st_release_gpu(a.flags + b, (unsigned)(t + 1));
-        if (t + 1 == a.n_steps) break;
-        if (tid < 4) {
-            const int nbx = bx + (tid == 0 ? -1 : tid == 1 ? 1 : 0), nby = by + (tid == 2 ? -1 : tid == 3 ? 1 : 0);
-            if (nbx >= 0 && nbx < a.tiles_x && nby >= 0 && nby < a.tiles_y) {
-                const unsigned* f = a.flags + nby * a.tiles_x + nbx;
-                const long long t0 = global_ns();
-                while (ld_acquire_gpu(f) < (unsigned)(t + 1)) {
-                    if (global_ns() - t0 > RS_TIMEOUT_NS) {
-                        *s_fail = 1;
-                        atomicExch(a.err, 1);
-                        break;
-                    }
-                }
-            }
-        }
-        __syncthreads();
-        if (*s_fail) {
-            failed = true;
-            break;
-        }
-        // the neighbours' boundary columns at the new state into the ring: RS_BATCH loads in flight
-        // per thread before their shared-memory stores
-        const int nring = (2 * ty + 2 * tx) * Gs;
-        for (int i0 = tid; i0 < nring; i0 += RS_BATCH * RS_THREADS) {
-            float4 val[RS_BATCH];
-            int dst[RS_BATCH];
-#pragma unroll
-            for (int q = 0; q < RS_BATCH; ++q) {
-                const int i = i0 + q * RS_THREADS;
-                dst[q] = -1;
-                val[q] = z4;
-                if (i < nring) {
-                    const int g = i % Gs, r = i / Gs;
-                    int lx, ly;
-                    if (r < 2 * ty) {
-                        lx = (r < ty) ? 0 : tx + 1;
-                        ly = (r % ty) + 1;
-                    } else {
-                        const int r2 = r - 2 * ty;
-                        ly = (r2 < tx) ? 0 : ty + 1;
-                        lx = (r2 % tx) + 1;
-                    }
-                    const int x = x0 + lx - 1, y = y0 + ly - 1;
-                    if (x >= 0 && x < nx && y >= 0 && y < ny) {
-                        dst[q] = (lx * row + ly) * RS_G + g;
-                        val[q] = __ldcg(reinterpret_cast<const float4*>(gnxt + gidx(x, y, 4 * g)));
-                    }
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < RS_BATCH; ++q)
-                if (dst[q] >= 0) Cs4[dst[q]] = val[q];
-        }
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < RS_R; ++r) {
-            cw[r] = Cs4[base + r * RS_G];
-            cc[r] = Cs4[base + PS + r * RS_G];
-        }
-    }
-    if (failed) return;
-    // the tile's final state (z < zs; deeper voxels are already in this buffer)
-    float* out = (a.n_steps & 1) ? a.buf1 : a.buf0;
-    for (int i = tid; i < tx * ty * Gs; i += RS_THREADS) {
-        const int g = i % Gs, col = i / Gs, y = col % ty, px = col / ty;
-        *reinterpret_cast<float4*>(out + gidx(x0 + px, y0 + y, 4 * g)) = Cs4[((px + 1) * row + y + 1) * RS_G + g];
-    }
-}
-
-struct ResidentPlan {
-    bool ok = false;
-    int tiles_x = 0, tiles_y = 0, grid = 0;
-};
-
-// The resident kernel runs when nz % 4 == 0 and one CTA per tile fits on the GPU at once.
-static ResidentPlan resident_plan(int nx, int ny, int nz) {
-    ResidentPlan r;
-    if (nz % 4 != 0) return r;
-    int dev = 0, sms = 0, occ = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return r;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return r;
-    r.tiles_x = (nx + RS_TX - 1) / RS_TX;
-    r.tiles_y = (ny + RS_TY - 1) / RS_TY;
-    r.grid = r.tiles_x * r.tiles_y;
-    if (r.grid > sms || r.grid > kPlumeMaxTiles) return r;
-    if (cudaFuncSetAttribute(k_plume_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS_SMEM) !=
-        cudaSuccess)
-        return r;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_plume_resident, RS_THREADS, RS_SMEM) != cudaSuccess ||
-        occ < 1)
-        return r;
-    r.ok = true;
-    return r;
-}
-
-bool plume_resident_active(const BdPlumeParams* p) {
-    return tune_value(BD_TUNE_PLUME_KERNEL) == BD_PLUME_KERNEL_RESIDENT && resident_plan(p->nx, p->ny, p->nz).ok;
-}
-
-// per-CTA step flags of the resident kernel, after the z lists in the plume scratch buffer
-static unsigned* resident_flags(uint8_t* mask, int nx, int ny, int nz) {
-    return reinterpret_cast<unsigned*>(mask + plume_flags_offset(nx, ny, nz));
-}
-
 int plume_policy_steps(const BdPlumeParams* p, int* n_steps, float* dt_step, float* decay_step) {
     const double idx2 = 1.0 / ((double)p->dx * p->dx), idy2 = 1.0 / ((double)p->dy * p->dy);
     const double idz2 = 1.0 / ((double)p->dz * p->dz);
@@ -894,7 +605,7 @@ static int compact_slots() {
 // non-void voxels may hold anything) the mask covers the whole grid and the non-void voxels of both
 // buffers are set to 0 first (every step keeps them 0).
 int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, const uint8_t* F, int* in_b,
-                 cudaStream_t st, const int* zlimit, int full_first, uint8_t* mask, int* err) {
+                 cudaStream_t st, const int* zlimit, int full_first, uint8_t* mask) {
     int steps;
     float dtp, decay;
     int rc = plume_policy_steps(p, &steps, &dtp, &decay);
@@ -919,31 +630,6 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
     }
     const long long total = (long long)steps * n_substeps;
     const int kernel = tune_value(BD_TUNE_PLUME_KERNEL);
-    if (kernel == BD_PLUME_KERNEL_RESIDENT && total <= (1LL << 30)) {
-        const ResidentPlan plan = resident_plan(nx, ny, nz);
-        if (plan.ok) {
-            ResidentArgs a;
-            a.buf0 = Ca; a.buf1 = Cb;
-            a.M = mask; a.zlimit = zl; a.flags = resident_flags(mask, nx, ny, nz); a.err = err;
-            a.nx = nx; a.ny = ny; a.nz = nz; a.mz = mz;
-            a.tiles_x = plan.tiles_x; a.tiles_y = plan.tiles_y; a.n_steps = (int)total;
-            a.k = tab;
-            BD_CUDA(cudaMemsetAsync(a.flags, 0, sizeof(unsigned) * plan.grid, st));
-            cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3(plan.grid);
-            cfg.blockDim = dim3(RS_THREADS);
-            cfg.dynamicSmemBytes = RS_SMEM;
-            cfg.stream = st;
-            cudaLaunchAttribute attr[1];
-            attr[0].id = cudaLaunchAttributeCooperative;
-            attr[0].val.cooperative = 1;
-            cfg.attrs = attr;
-            cfg.numAttrs = 1;
-            BD_CUDA(cudaLaunchKernelEx(&cfg, k_plume_resident, a));
-            if (in_b) *in_b = (int)(total & 1);
-            return BD_OK;
-        }
-    }
     const bool vec = nz % 4 == 0;  // the direct kernels move float4 groups
     if (kernel == BD_PLUME_KERNEL_COMPACT && vec && (nz + 3) / 4 <= 255) {
         const int n_yt = (ny + PD_BY - 1) / PD_BY;
@@ -1222,21 +908,14 @@ extern "C" int bd_plume_advance(const BdPlumeParams* p, float* Ca, float* Cb, in
         return BD_OK;
     }
     cudaStream_t st = as_stream(stream);
-    unsigned char* scratch = nullptr;  // plume neighbourhood bytes + a 4-byte error flag
-    const size_t flag_off = plume_mask_bytes(p->nx, p->ny, p->nz);
-    BD_CUDA(cudaMallocAsync((void**)&scratch, flag_off + 16, st));
-    int* err = reinterpret_cast<int*>(scratch + flag_off);
-    int rc = BD_OK;
-    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), st);
-    if (e == cudaSuccess) rc = plume_launch(p, Ca, Cb, n_substeps, F, in_b, st, nullptr, 1, scratch, err);
-    int host_err = 0;
-    if (e == cudaSuccess && rc == BD_OK) e = cudaMemcpyAsync(&host_err, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    unsigned char* scratch = nullptr;  // plume neighbourhood bytes, z lists and unit lists
+    BD_CUDA(cudaMallocAsync((void**)&scratch, plume_mask_bytes(p->nx, p->ny, p->nz), st));
+    const int rc = plume_launch(p, Ca, Cb, n_substeps, F, in_b, st, nullptr, 1, scratch);
     cudaError_t e2 = cudaFreeAsync(scratch, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaError_t e = cudaStreamSynchronize(st);
     if (rc) return rc;
     if (e != cudaSuccess) return cuda_status(e, "bd_plume_advance");
     if (e2 != cudaSuccess) return cuda_status(e2, "bd_plume_advance: cudaFreeAsync");
-    if (host_err) return fail(BD_ERR_TIMEOUT, "bd_plume_advance: a bounded wait of the resident plume kernel timed out");
     return BD_OK;
 }
 

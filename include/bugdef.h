@@ -376,18 +376,10 @@ BD_API int bd_engine_record(BdEngine* e, const BdRecordSpec* spec, void* slot, v
                                         limit); photons per thread = n_photons / (grid * 128)          */
 #define BD_TUNE_STENCIL_XC        1  /* x-planes per CTA of the TMA substep kernel, 1..64 (default 8)   */
 #define BD_TUNE_PLUME_XC          2  /* direct plume kernel: x-planes per CTA, 1..64 (default 4)         */
-#define BD_TUNE_PLUME_KERNEL      3  /* plume stage: BD_PLUME_KERNEL_DIRECT (default),
-                                        BD_PLUME_KERNEL_RESIDENT or BD_PLUME_KERNEL_COMPACT             */
+#define BD_TUNE_PLUME_KERNEL      3  /* plume stage: BD_PLUME_KERNEL_DIRECT (default) or
+                                        BD_PLUME_KERNEL_COMPACT (value 5 is not used)                   */
 #define BD_PLUME_KERNEL_DIRECT    4  /* one launch per FTCS step: a CTA per 32 (z) x 16 (y) tile column
                                         marching x planes over the column's live z groups              */
-#define BD_PLUME_KERNEL_RESIDENT  5  /* one launch per stage: a persistent CTA per column tile (at most
-                                        15 x 20) keeps its tile in shared memory for every step and
-                                        swaps a one-voxel halo with its neighbours through L2 (measured
-                                        slower than the direct kernel on the full-resolution run). It
-                                        holds every SM for the stage, so stages of engines that run on
-                                        other streams at the same time must use the direct kernel.
-                                        Grids whose tiles exceed the SMs, or nz % 4 != 0, fall back to
-                                        the direct kernel                                              */
 #define BD_PLUME_KERNEL_COMPACT   6  /* the direct kernel's per-unit code over a compact list of the live
                                         (column, band) units, one wave of CTAs per step: once per stage
                                         the x planes per unit are chosen on the device (2..12, the

@@ -34,7 +34,7 @@ def test_knob_validation(gpu, restore_knobs):
         _knob(_lib.TUNE_STENCIL_XC, 0)
     with pytest.raises(ValueError):
         _knob(_lib.TUNE_MC_BLOCKS_PER_SM, 17)
-    for bad in (0, 3, 7):
+    for bad in (0, 3, 5, 7):
         with pytest.raises(ValueError):
             _knob(_lib.TUNE_PLUME_KERNEL, bad)
     for bad in (-1, 17):
@@ -68,12 +68,11 @@ def test_launch_shapes_leave_results_bit_identical(gpu, restore_knobs):
 
 
 def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
-    """Every plume kernel gives the same bits: the resident kernel (one launch per stage, tiles
-    kept in shared memory, halos swapped between CTAs; z >= 128 updated from global memory) and the
-    direct kernel in both unit orders (several x-chunk lengths), through the context API (arbitrary values in non-void
-    voxels, ragged y tiles, scattered void, a partly filled last z tile, columns deeper than the
-    shared-memory part) and through the engine (void z-limit, partly void voxel groups at the crater
-    walls, bulk-void fast path)."""
+    """Every plume kernel gives the same bits: the direct kernel in both unit orders (grid over the
+    z-list columns with several x-chunk lengths, and the compact unit list), through the context API
+    (arbitrary values in non-void voxels, ragged y tiles, scattered void, a partly filled last z
+    tile, deep cavities under trimmed and empty columns) and through the engine (void z-limit, partly
+    void voxel groups at the crater walls, bulk-void fast path)."""
     from bug_defense_b200 import _lib, campaign
     rng = np.random.default_rng(11)
     scattered = rng.uniform(size=(9, 35, 68)) < 0.7
@@ -91,7 +90,7 @@ def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
         C0 = (rng.uniform(0, 1, shape) * vd).astype(np.float32)
         z = np.zeros(shape)
         fields = []
-        for kern, xc in ((5, 4), (4, 2), (4, 1), (4, 3), (4, 4), (6, 4)):
+        for kern, xc in ((4, 2), (4, 1), (4, 3), (4, 4), (6, 4)):
             _knob(_lib.TUNE_PLUME_KERNEL, kern)
             _knob(_lib.TUNE_PLUME_XC, xc)
             ctx = gpu.MetalAblationContext(*shape, 0.03, 0.025, 0.02, 1e-5, 0.0, 20.0, 100.0, 300.0,
@@ -106,7 +105,7 @@ def test_plume_kernel_shapes_leave_results_bit_identical(gpu, restore_knobs):
         assert np.any(fields[0] != C0)
     inst = _small(22)                                  # 2940 nm, 80 W: a crater opens
     runs = []
-    for kern in (5, 4, 6):
+    for kern in (4, 6):
         _knob(_lib.TUNE_PLUME_KERNEL, kern)
         camp = campaign.Campaign([inst])
         camp.run(14, sync_every=14)
@@ -150,17 +149,16 @@ def _small(index, photons=20_000):
     return dict(inst, n_photons=photons, pulse_ms=12.0)
 
 
-@pytest.mark.parametrize("kern,batch", [(4, True), (4, False), (5, False)],
-                         ids=["batched-plume", "direct-streams", "resident-one-stream"])
+@pytest.mark.parametrize("kern,batch", [(4, True), (4, False), (6, False)],
+                         ids=["batched-plume", "direct-streams", "compact-streams"])
 def test_concurrent_campaign_equals_instances_run_alone(gpu, restore_knobs, kern, batch):
     """Instances run together give the bits of each instance run alone with its own plume stage:
-    with the batched plume stage (one launch per FTCS step over every instance's units), with each
-    instance's stages on its own stream, and with the resident kernel on one shared stream."""
+    with the batched plume stage (one launch per FTCS step over every instance's units), and with
+    each instance's stages on its own stream (direct and compact plume kernels)."""
     from bug_defense_b200 import _lib, campaign
     _knob(_lib.TUNE_PLUME_KERNEL, kern)
     insts = [_small(i) for i in (1, 10, 23)]           # 532, 1064 and 2940 nm
     camp = campaign.Campaign(insts, batch_plume=batch)
-    assert camp.shared_stream == (kern == _lib.PLUME_KERNEL_RESIDENT)
     assert (camp.batch is not None) == batch
     camp.run(30, sync_every=10)
     together = [(e.T.copy(), e.ablated.copy(), e.H_acc.copy(), e.plume.raw.double().cpu().numpy())
@@ -181,7 +179,7 @@ def test_autotune_sets_the_fastest_candidates(gpu, restore_knobs):
     from bug_defense_b200 import _lib, campaign
     res = campaign.autotune(_small(4), epochs_per_trial=2,
                             candidates={_lib.TUNE_MC_BLOCKS_PER_SM: [2, 4], _lib.TUNE_STENCIL_XC: [4, 8],
-                                        _lib.TUNE_PLUME_KERNEL: [4, 6, 5], _lib.TUNE_PLUME_XC: [2, 4],
+                                        _lib.TUNE_PLUME_KERNEL: [4, 6], _lib.TUNE_PLUME_XC: [2, 4],
                                         _lib.TUNE_STENCIL_CAP: [0, 2]})
     for name, knob in (("mc_ctas_per_sm", _lib.TUNE_MC_BLOCKS_PER_SM), ("stencil_xc", _lib.TUNE_STENCIL_XC),
                        ("stencil_cap", _lib.TUNE_STENCIL_CAP)):
@@ -189,9 +187,9 @@ def test_autotune_sets_the_fastest_candidates(gpu, restore_knobs):
         assert [v for v, _ in trials] == sorted(v for v, _ in trials) and all(t > 0 for _, t in trials)
         assert res[name] == min(trials, key=lambda t: t[1])[0] == _knob(knob)
     # the plume kernel and the direct kernel's x-planes are searched together; the compact kernel
-    # picks its x-planes per stage and the resident kernel has none
+    # picks its x-planes per stage
     plume = res["trials"]["plume"]
-    assert [(k, x) for k, x, _ in plume] == [(4, 2), (4, 4), (6, None), (5, None)]
+    assert [(k, x) for k, x, _ in plume] == [(4, 2), (4, 4), (6, None)]
     assert all(t > 0 for _, _, t in plume)
     k, x, _ = min(plume, key=lambda t: t[2])
     assert res["plume_kernel"] == k == _knob(_lib.TUNE_PLUME_KERNEL)
