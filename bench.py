@@ -438,6 +438,19 @@ def ours_main(args):
             mc["photon_steps_per_s"] = steps_per_epoch * r["n_on"] / (mc_ms * 1e-3)
         lc = (ld[1:7].sum() + ld[8] + ld[9] - ld[7]) / max(ld[0], 1)
         mc["ledger_closure_minus_1"] = float(lc - 1.0)
+        # issue-rate roof: SMs x 4 schedulers x 1 warp instruction per clock x 32 lanes / thread
+        # instructions per photon-step (the count of one ncu capture, profiles/traffic.json)
+        tf = ROOT / "profiles" / "traffic.json"
+        ipp = json.loads(tf.read_text()).get("k_mc_trace", {}).get("thread_instructions_per_photon_step") \
+            if tf.exists() else None
+        if ipp and mc_ms > 0:
+            import torch
+            n_sm = torch.cuda.get_device_properties(eng.dev).multi_processor_count
+            mhz = (r["clocks"] or {}).get("sm_mhz") or 1965.0
+            roof_steps = n_sm * 4 * mhz * 1e6 * 32 / ipp
+            mc["issue_roof_photon_steps_per_s"] = roof_steps
+            mc["issue_roof_frac"] = round(mc["photon_steps_per_s"] / roof_steps, 4)
+            mc["thread_instructions_per_photon_step"] = ipp
     # per epoch: begin + 3 epoch-end kernels + plume mask + plume z lists + substeps + plume steps;
     # per laser epoch: MC, ledger reduction and tally finalisation
     gpu_launches = K * (1 + 3 + 2 + eng.n_substeps + eng.n_substeps * n_plume_sub) + r["n_on"] * 3

@@ -81,3 +81,44 @@ def test_engine_mc_epoch_runs_and_conserves_energy(gpu, golden):
     assert np.max(eng.T) > cfg['t_ambient']
     assert eng.Q.shape == eng.ablated.shape and np.all(eng.Q >= 0)
     assert eng.last_mc['engine'] == 'gpu'
+
+
+def test_layered_host_grids_build_the_same_engine(gpu):
+    """Host grids that are one z column broadcast over x and y cross PCIe as that column; an engine
+    built from them holds the same bits as one built from the same grids passed as device tensors
+    (copied whole), before and after laser epochs. A grid with one changed voxel is copied whole."""
+    import torch
+    from bug_defense_b200 import _device
+    from bug_defense_b200.workloads import engine_kwargs, full_coupled_run
+    geo = full_coupled_run(seed=3, nx=32, ny=24, nz=128, n_plume_air=8)
+    geo["optical"]["mu_s"][5, 7, 100] *= 1.5            # one grid that is not layered
+    kw_host = engine_kwargs(geo)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    def on_dev(v):
+        if isinstance(v, np.ndarray):
+            return torch.as_tensor(v, device=dev)
+        if isinstance(v, dict):
+            return {k: on_dev(x) for k, x in v.items()}
+        return v
+
+    kw_dev = {k: on_dev(v) for k, v in kw_host.items()}
+    before = dict(_device.upload_stats)
+    eh = gpu.CoupledAblationEngine(**kw_host, device=dev)
+    cols = _device.upload_stats["column_grids"] - before["column_grids"]
+    fulls = _device.upload_stats["full_grids"] - before["full_grids"]
+    assert cols == 14 and fulls == 1, (cols, fulls)
+    ed = gpu.CoupledAblationEngine(**kw_dev, device=dev)
+
+    def state(e):
+        out = [e._opt_t[k] for k in ("mu_a", "mu_s", "g", "n")] + [e._k, e._rho, e._h_lat, e._flags, e._T]
+        out += list(e._wet) + [e._ds_t[k] for k in sorted(e._ds_t)] + [e._props, e.plume.raw]
+        return [t.detach().clone() for t in out]
+
+    for a, b in zip(state(eh), state(ed)):
+        assert torch.equal(a.view(torch.uint8), b.view(torch.uint8))
+    for e in (eh, ed):
+        e.step_epochs(3)
+    for a, b in zip(state(eh), state(ed)):
+        assert torch.equal(a.view(torch.uint8), b.view(torch.uint8))
+    assert float(eh._T.max()) > 30.0
