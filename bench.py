@@ -259,6 +259,8 @@ def run_ours(args, rank, world, local):
             cand = {_lib.TUNE_PLUME_KERNEL: [args.plume_kernel]}
         tuned = campaign.autotune(probe, candidates=cand)
         torch.cuda.synchronize()
+        if rank == 0:
+            print("autotune trials (ms per epoch):", json.dumps(tuned["trials"]), file=sys.stderr)
     if args.plume_kernel is not None:
         _lib.call("bd_tune_set", _lib.TUNE_PLUME_KERNEL, args.plume_kernel)
     from bug_defense_b200.replicas import replica_seed
