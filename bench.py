@@ -501,7 +501,7 @@ def denoiser_leg():
 
 
 def denoised_run_leg(n_laser=10, check_every=5):
-    """the 532 nm and 1470 nm, 40 W runs at full resolution, laser-on epochs timed on the
+    """The denoised coupled run: the 532 nm and 1470 nm, 40 W runs at full resolution, laser-on epochs timed on the
     device with plain 150k-photon MC and with 15k photons through the denoiser (spot-checked against
     plain MC every `check_every` laser epochs), each on a fresh engine after 3 warm-up epochs."""
     import torch

@@ -64,8 +64,8 @@ def _executor() -> ThreadPoolExecutor:
 def slice_column(arr: np.ndarray):
     """The z column c when a C-order (nx, ny, nz) grid holds c at every (x, y), else None.
 
-    Layered stacks are built that way: the production runner's geometry and the configs' stacks
-    give every property per z slice and broadcast it over x and y
+    Layered stacks are built that way: the production runner's geometry and the seeded benchmark
+    stacks give every property per z slice and broadcast it over x and y
     (run_highres_knowledge_suite.py:126-185). Such a grid is uploaded as its column and expanded
     on the device, which moves nz values over PCIe instead of nx*ny*nz. The comparison is bitwise
     (the grid viewed as unsigned integers), so -0.0, NaN payloads and every other bit pattern are

@@ -1,4 +1,4 @@
-"""The denoised coupled run (configs[4] pattern, denoised.DenoisedCoupledRun) on a small stack: laser
+"""The denoised coupled run (denoised.DenoisedCoupledRun: 15k photons + U-Net) on a small stack: laser
 epochs take their source from a 15k-photon map through the trained network, spot checks compare it
 with the plain map, and a threshold below the observed distance falls back to plain MC for good."""
 import numpy as np
