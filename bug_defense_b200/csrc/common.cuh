@@ -38,14 +38,15 @@ inline size_t plume_zlist_bytes(int nx, int ny, int nz) {
 }
 // Then the compact-order state of the direct plume kernel: 16 header words (unit count, chosen
 // x planes per unit, unit count per candidate), the live-group bitmaps of every (x plane, y tile)
-// (8 words each), then the units (column << 5 | band), at most one per band of every column.
+// (8 words each), then the units (16 bytes: column << 5 | band and the band's 8 group ids), at
+// most one per band of every column.
 inline size_t plume_units_offset(int nx, int ny, int nz) {
     return plume_zlist_offset(nx, ny, nz) + plume_zlist_bytes(nx, ny, nz);
 }
 inline size_t plume_units_bytes(int nx, int ny, int nz) {
     const size_t cols = (size_t)nx * ((ny + kPlumeZRows - 1) / kPlumeZRows);
     const size_t bands = ((size_t)(nz + 3) / 4 + 7) / 8;
-    return ((16 + cols * 8 + cols * bands) * sizeof(unsigned) + 255) / 256 * 256;
+    return ((16 + cols * 8) * sizeof(unsigned) + cols * bands * 16 + 255) / 256 * 256;
 }
 inline size_t plume_mask_bytes(int nx, int ny, int nz) {
     return plume_units_offset(nx, ny, nz) + plume_units_bytes(nx, ny, nz);

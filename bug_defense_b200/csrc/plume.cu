@@ -318,17 +318,15 @@ __global__ void __launch_bounds__(256) k_plume_zlist(const uint8_t* __restrict__
 // groups, so z tiles that are partly tissue cost only their void groups. A lane whose z neighbour
 // group is not held by the neighbouring lane loads that neighbour voxel instead of taking it by
 // shuffle. Voxels outside the lists are not void and are never written. Uniform over the CTA.
-__device__ __forceinline__ void plume_direct_unit(const float* __restrict__ C, float* __restrict__ Cn,
+// g: this lane's z group (-2 when the band has no group for the lane); uniform early exit over the
+// CTA when the x chunk is empty.
+__device__ __forceinline__ void plume_unit_groups(const float* __restrict__ C, float* __restrict__ Cn,
                                                   const uint8_t* __restrict__ M, int nx, int ny, int nz, int mz,
-                                                  int xc, const PlumeTab& k, int zl, const uint8_t* __restrict__ zlist,
-                                                  int n_cols, int col, int yt, int xch, int band, const float* w0s) {
-    const int G = (nz + 3) / 4;
-    const int cnt = zlist[col];
-    const int b0 = band * 8;
+                                                  int xc, const PlumeTab& k, int zl, int g, int yt, int xch,
+                                                  const float* w0s) {
     const int ib = xch * xc, ie = min(nx, ib + xc);
-    if (b0 >= cnt || ib >= ie) return;
+    if (ib >= ie) return;
     const int zg = threadIdx.x & 7;
-    const int g = b0 + zg < cnt ? (int)zlist[n_cols + col * G + b0 + zg] : -2;
     const int gp = __shfl_up_sync(0xffffffffu, g, 1, 8);
     const int gn = __shfl_down_sync(0xffffffffu, g, 1, 8);
     const bool zb_lane = zg > 0 && gp == g - 1;  // the -z neighbour is the previous lane's last voxel
@@ -368,6 +366,20 @@ __device__ __forceinline__ void plume_direct_unit(const float* __restrict__ C, f
     }
 }
 
+// The unit (column col, band) with its groups read from the column's z list.
+__device__ __forceinline__ void plume_direct_unit(const float* __restrict__ C, float* __restrict__ Cn,
+                                                  const uint8_t* __restrict__ M, int nx, int ny, int nz, int mz,
+                                                  int xc, const PlumeTab& k, int zl, const uint8_t* __restrict__ zlist,
+                                                  int n_cols, int col, int yt, int xch, int band, const float* w0s) {
+    const int G = (nz + 3) / 4;
+    const int cnt = zlist[col];
+    const int b0 = band * 8;
+    if (b0 >= cnt) return;  // uniform over the CTA
+    const int zg = threadIdx.x & 7;
+    const int g = b0 + zg < cnt ? (int)zlist[n_cols + col * G + b0 + zg] : -2;
+    plume_unit_groups(C, Cn, M, nx, ny, nz, mz, xc, k, zl, g, yt, xch, w0s);
+}
+
 // BD_PLUME_KERNEL_DIRECT: grid (bands, y tiles, x chunks); CTAs past a column's live bands exit at once.
 __global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_z(const float* __restrict__ C, float* __restrict__ Cn,
                                                                  const uint8_t* __restrict__ M, int nx, int ny,
@@ -393,7 +405,8 @@ __global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_z(const float* __
 // wins (fewer planes per unit = a shorter CTA). The z list and the unit list are then built for it
 // and the step kernel, one wave of CTAs, loops over the units. Region layout (32-bit words, from
 // plume_units_offset): [0] unit count, [1] chosen xc, [4 + c - kPlumeXcMin] unit count for xc = c,
-// then the bitmaps (nx x y tiles x kPlumeBitWords), then the units (column << 5 | band).
+// then the bitmaps (nx x y tiles x kPlumeBitWords), then the units: 16 bytes each, {column << 5 |
+// band, 0, the band's 8 z-group ids as bytes (0xFF: none)}.
 constexpr int kPlumeXcMin = 2, kPlumeXcMax = 12;
 constexpr int kPlumeBitWords = 8;  // 32-group words of a bitmap: 4-voxel groups <= 255
 constexpr int kPlumeHdrWords = 16;
@@ -491,8 +504,8 @@ __global__ void __launch_bounds__(256) k_plume_zlist_bits(const unsigned* __rest
 
 // the unit list of the chosen xc's columns, in column order: one CTA, a block-wide exclusive scan
 // of the bands per column
-__global__ void __launch_bounds__(1024) k_plume_units(const uint8_t* __restrict__ zlist, int nx, int n_yt,
-                                                      unsigned* __restrict__ hdr, unsigned* __restrict__ units) {
+__global__ void __launch_bounds__(1024) k_plume_units(const uint8_t* __restrict__ zlist, int nx, int n_yt, int G,
+                                                      unsigned* __restrict__ hdr, uint4* __restrict__ units) {
     __shared__ int part[32];
     __shared__ int base;
     if (threadIdx.x == 0) base = 0;
@@ -520,7 +533,19 @@ __global__ void __launch_bounds__(1024) k_plume_units(const uint8_t* __restrict_
         }
         __syncthreads();
         const int excl = base + (w > 0 ? part[w - 1] : 0) + v - nb;
-        for (int b = 0; b < nb; ++b) units[excl + b] = ((unsigned)col << 5) | (unsigned)b;
+        for (int b = 0; b < nb; ++b) {
+            // the band's group ids, one byte per lane (0xFF: no group), so that a step's CTA learns
+            // its unit with one 16-byte load
+            const uint8_t* gl = zlist + n_cols + (size_t)col * G + 8 * b;
+            const int n_in = min(8, (int)zlist[col] - 8 * b);
+            unsigned lo = 0u, hi = 0u;
+            for (int q = 0; q < 8; ++q) {
+                const unsigned gq = q < n_in ? (unsigned)gl[q] : 0xFFu;
+                if (q < 4) lo |= gq << (8 * q);
+                else hi |= gq << (8 * (q - 4));
+            }
+            units[excl + b] = make_uint4(((unsigned)col << 5) | (unsigned)b, 0u, lo, hi);
+        }
         __syncthreads();
         if (threadIdx.x == 1023) base = excl + nb;
         __syncthreads();
@@ -533,22 +558,22 @@ __global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_c(const float* __
                                                                  const uint8_t* __restrict__ M, int nx, int ny,
                                                                  int nz, int mz, const __grid_constant__ PlumeTab k,
                                                                  const int* __restrict__ zlimit,
-                                                                 const uint8_t* __restrict__ zlist,
                                                                  const unsigned* __restrict__ hdr,
-                                                                 const unsigned* __restrict__ units, int n_yt) {
+                                                                 const uint4* __restrict__ units, int n_yt) {
     __shared__ float w0s[64];
     if (threadIdx.x < 64) w0s[threadIdx.x] = k.w0eff[threadIdx.x];
     __syncthreads();
     const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
     const int nu = (int)__ldg(&hdr[0]);
     const int xc = (int)__ldg(&hdr[1]);
-    const int n_cols = n_yt * ((nx + xc - 1) / xc);
+    const int zg = threadIdx.x & 7;
     for (int u = blockIdx.x; u < nu; u += gridDim.x) {
-        const unsigned v = __ldg(&units[u]);
-        const int col = (int)(v >> 5);
+        const uint4 r = __ldg(&units[u]);  // column << 5 | band, then the band's 8 group ids
+        const int col = (int)(r.x >> 5);
         const int xch = col / n_yt;
-        plume_direct_unit(C, Cn, M, nx, ny, nz, mz, xc, k, zl, zlist, n_cols, col, col - xch * n_yt, xch,
-                          (int)(v & 31u), w0s);
+        const unsigned gb = ((zg < 4 ? r.z : r.w) >> (8 * (zg & 3))) & 0xFFu;
+        plume_unit_groups(C, Cn, M, nx, ny, nz, mz, xc, k, zl, gb == 0xFFu ? -2 : (int)gb, col - xch * n_yt, xch,
+                          w0s);
     }
 }
 
@@ -635,20 +660,19 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
         const int n_yt = (ny + PD_BY - 1) / PD_BY;
         unsigned* hdr = reinterpret_cast<unsigned*>(mask + plume_units_offset(nx, ny, nz));
         unsigned* bits = hdr + kPlumeHdrWords;
-        unsigned* units = bits + (size_t)nx * n_yt * kPlumeBitWords;
+        uint4* units = reinterpret_cast<uint4*>(bits + (size_t)nx * n_yt * kPlumeBitWords);
         uint8_t* zlist = mask + plume_zlist_offset(nx, ny, nz);
         const int slots = compact_slots();
         k_plume_planebits<<<dim3(n_yt, nx), 256, 0, st>>>(mask, nx, ny, nz, mz, zl, bits);
         k_plume_unit_counts<<<kPlumeXcMax - kPlumeXcMin + 1, 1024, 0, st>>>(bits, nx, n_yt, (nz + 3) / 4, hdr);
         k_plume_pick_xc<<<1, 32, 0, st>>>(hdr, slots + slots * 3 / 100);
         k_plume_zlist_bits<<<dim3(n_yt, (nx + kPlumeXcMin - 1) / kPlumeXcMin), 256, 0, st>>>(bits, nx, nz, hdr, zlist);
-        k_plume_units<<<1, 1024, 0, st>>>(zlist, nx, n_yt, hdr, units);
+        k_plume_units<<<1, 1024, 0, st>>>(zlist, nx, n_yt, (nz + 3) / 4, hdr, units);
         BD_CHECK_LAUNCH("k_plume_units");
         for (long long s = 0; s < total; ++s) {
             const float* in = (s & 1) ? Cb : Ca;
             float* out = (s & 1) ? Ca : Cb;
-            k_plume_direct_c<<<slots, 8 * PD_BY, 0, st>>>(in, out, mask, nx, ny, nz, mz, tab, zl, zlist, hdr, units,
-                                                           n_yt);
+            k_plume_direct_c<<<slots, 8 * PD_BY, 0, st>>>(in, out, mask, nx, ny, nz, mz, tab, zl, hdr, units, n_yt);
         }
         BD_CHECK_LAUNCH("k_plume_direct_c");
         if (in_b) *in_b = (int)(total & 1);
