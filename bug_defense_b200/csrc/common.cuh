@@ -43,10 +43,13 @@ inline size_t plume_zlist_bytes(int nx, int ny, int nz) {
 inline size_t plume_units_offset(int nx, int ny, int nz) {
     return plume_zlist_offset(nx, ny, nz) + plume_zlist_bytes(nx, ny, nz);
 }
+inline size_t plume_unit_capacity(int nx, int ny, int nz) {
+    const size_t cols = (size_t)nx * ((ny + kPlumeZRows - 1) / kPlumeZRows);
+    return cols * (((size_t)(nz + 3) / 4 + 7) / 8);
+}
 inline size_t plume_units_bytes(int nx, int ny, int nz) {
     const size_t cols = (size_t)nx * ((ny + kPlumeZRows - 1) / kPlumeZRows);
-    const size_t bands = ((size_t)(nz + 3) / 4 + 7) / 8;
-    return ((16 + cols * 8) * sizeof(unsigned) + cols * bands * 16 + 255) / 256 * 256;
+    return ((16 + cols * 8) * sizeof(unsigned) + plume_unit_capacity(nx, ny, nz) * 16 + 255) / 256 * 256;
 }
 inline size_t plume_mask_bytes(int nx, int ny, int nz) {
     return plume_units_offset(nx, ny, nz) + plume_units_bytes(nx, ny, nz);

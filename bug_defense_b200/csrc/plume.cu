@@ -559,16 +559,21 @@ __global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_c(const float* __
                                                                  int nz, int mz, const __grid_constant__ PlumeTab k,
                                                                  const int* __restrict__ zlimit,
                                                                  const unsigned* __restrict__ hdr,
-                                                                 const uint4* __restrict__ units, int n_yt) {
+                                                                 const uint4* __restrict__ units, int n_yt,
+                                                                 int unit_cap) {
+    // the CTA's first unit record is loaded beside the header (not after the unit count is known):
+    // one L2 round trip before the field loads; a record past the count is never used
+    const uint4 r0 = __ldg(&units[min((int)blockIdx.x, unit_cap - 1)]);
+    const int nu = (int)__ldg(&hdr[0]);
+    const int xc = (int)__ldg(&hdr[1]);
+    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
     __shared__ float w0s[64];
     if (threadIdx.x < 64) w0s[threadIdx.x] = k.w0eff[threadIdx.x];
     __syncthreads();
-    const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
-    const int nu = (int)__ldg(&hdr[0]);
-    const int xc = (int)__ldg(&hdr[1]);
     const int zg = threadIdx.x & 7;
     for (int u = blockIdx.x; u < nu; u += gridDim.x) {
-        const uint4 r = __ldg(&units[u]);  // column << 5 | band, then the band's 8 group ids
+        // column << 5 | band, then the band's 8 group ids
+        const uint4 r = u == (int)blockIdx.x ? r0 : __ldg(&units[u]);
         const int col = (int)(r.x >> 5);
         const int xch = col / n_yt;
         const unsigned gb = ((zg < 4 ? r.z : r.w) >> (8 * (zg & 3))) & 0xFFu;
@@ -661,6 +666,7 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
         unsigned* hdr = reinterpret_cast<unsigned*>(mask + plume_units_offset(nx, ny, nz));
         unsigned* bits = hdr + kPlumeHdrWords;
         uint4* units = reinterpret_cast<uint4*>(bits + (size_t)nx * n_yt * kPlumeBitWords);
+        const int unit_cap = (int)plume_unit_capacity(nx, ny, nz);
         uint8_t* zlist = mask + plume_zlist_offset(nx, ny, nz);
         const int slots = compact_slots();
         k_plume_planebits<<<dim3(n_yt, nx), 256, 0, st>>>(mask, nx, ny, nz, mz, zl, bits);
@@ -672,7 +678,8 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
         for (long long s = 0; s < total; ++s) {
             const float* in = (s & 1) ? Cb : Ca;
             float* out = (s & 1) ? Ca : Cb;
-            k_plume_direct_c<<<slots, 8 * PD_BY, 0, st>>>(in, out, mask, nx, ny, nz, mz, tab, zl, hdr, units, n_yt);
+            k_plume_direct_c<<<slots, 8 * PD_BY, 0, st>>>(in, out, mask, nx, ny, nz, mz, tab, zl, hdr, units, n_yt,
+                                                           unit_cap);
         }
         BD_CHECK_LAUNCH("k_plume_direct_c");
         if (in_b) *in_b = (int)(total & 1);
