@@ -553,8 +553,11 @@ __global__ void __launch_bounds__(1024) k_plume_units(const uint8_t* __restrict_
     if (threadIdx.x == 0) hdr[0] = (unsigned)base;
 }
 
-// one step over the unit list: a wave of CTAs, CTA b runs units b, b + gridDim.x, ...
-__global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_c(const float* __restrict__ C, float* __restrict__ Cn,
+// One step over the unit list: a wave of CTAs, each running kPlumeUnitsPerCta units at a time, one per
+// 128-thread group (the groups share no barrier): group g of CTA b runs units 3b + g, 3b + g + 3 grid,
+// ... A step's wave is then dispatched as a third as many CTAs with the same resident threads per SM.
+constexpr int kPlumeUnitsPerCta = 3;
+__global__ void __launch_bounds__(8 * PD_BY * kPlumeUnitsPerCta, 3) k_plume_direct_c(const float* __restrict__ C, float* __restrict__ Cn,
                                                                  const uint8_t* __restrict__ M, int nx, int ny,
                                                                  int nz, int mz, const __grid_constant__ PlumeTab k,
                                                                  const int* __restrict__ zlimit,
@@ -563,7 +566,9 @@ __global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_c(const float* __
                                                                  int unit_cap) {
     // the CTA's first unit record is loaded beside the header (not after the unit count is known):
     // one L2 round trip before the field loads; a record past the count is never used
-    const uint4 r0 = __ldg(&units[min((int)blockIdx.x, unit_cap - 1)]);
+    const int grp = threadIdx.x >> 7;  // this thread's unit slot within the CTA
+    const int u0 = (int)blockIdx.x * kPlumeUnitsPerCta + grp;
+    const uint4 r0 = __ldg(&units[min(u0, unit_cap - 1)]);
     const int nu = (int)__ldg(&hdr[0]);
     const int xc = (int)__ldg(&hdr[1]);
     const int zl = zlimit ? min(max(*zlimit, 0), nz) : nz;
@@ -571,9 +576,9 @@ __global__ void __launch_bounds__(8 * PD_BY, 9) k_plume_direct_c(const float* __
     if (threadIdx.x < 64) w0s[threadIdx.x] = k.w0eff[threadIdx.x];
     __syncthreads();
     const int zg = threadIdx.x & 7;
-    for (int u = blockIdx.x; u < nu; u += gridDim.x) {
+    for (int u = u0; u < nu; u += gridDim.x * kPlumeUnitsPerCta) {
         // column << 5 | band, then the band's 8 group ids
-        const uint4 r = u == (int)blockIdx.x ? r0 : __ldg(&units[u]);
+        const uint4 r = u == u0 ? r0 : __ldg(&units[u]);
         const int col = (int)(r.x >> 5);
         const int xch = col / n_yt;
         const unsigned gb = ((zg < 4 ? r.z : r.w) >> (8 * (zg & 3))) & 0xFFu;
@@ -624,8 +629,8 @@ static int compact_slots() {
     if (v > 0) return v;
     int nsm = 0, per = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_plume_direct_c, 8 * PD_BY, 0);
-    v = std::max(1, nsm) * std::max(1, per);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_plume_direct_c, 8 * PD_BY * kPlumeUnitsPerCta, 0);
+    v = std::max(1, nsm) * std::max(1, per) * kPlumeUnitsPerCta;  // units of one wave
     cache[d].store(v);
     return v;
 }
@@ -678,8 +683,8 @@ int plume_launch(const BdPlumeParams* p, float* Ca, float* Cb, int n_substeps, c
         for (long long s = 0; s < total; ++s) {
             const float* in = (s & 1) ? Cb : Ca;
             float* out = (s & 1) ? Ca : Cb;
-            k_plume_direct_c<<<slots, 8 * PD_BY, 0, st>>>(in, out, mask, nx, ny, nz, mz, tab, zl, hdr, units, n_yt,
-                                                           unit_cap);
+            k_plume_direct_c<<<slots / kPlumeUnitsPerCta, 8 * PD_BY * kPlumeUnitsPerCta, 0, st>>>(
+                in, out, mask, nx, ny, nz, mz, tab, zl, hdr, units, n_yt, unit_cap);
         }
         BD_CHECK_LAUNCH("k_plume_direct_c");
         if (in_b) *in_b = (int)(total & 1);
