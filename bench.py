@@ -453,9 +453,11 @@ def ours_main(args):
             mc["issue_roof_photon_steps_per_s"] = roof_steps
             mc["issue_roof_frac"] = round(mc["photon_steps_per_s"] / roof_steps, 4)
             mc["thread_instructions_per_photon_step"] = ipp
-    # per epoch: begin + 3 epoch-end kernels + plume mask + plume z lists + substeps + plume steps;
-    # per laser epoch: MC, ledger reduction and tally finalisation
-    gpu_launches = K * (1 + 3 + 2 + eng.n_substeps + eng.n_substeps * n_plume_sub) + r["n_on"] * 3
+    # per epoch: begin + 3 epoch-end kernels + the plume stage's set-up (mask and z lists; with the
+    # compact kernel the mask, bitmaps, unit counts, x-planes pick, z lists and unit list) + substeps +
+    # plume steps; per laser epoch: MC, ledger reduction and tally finalisation
+    plume_prep = 6 if kv.value == _lib.PLUME_KERNEL_COMPACT else 2
+    gpu_launches = K * (1 + 3 + plume_prep + eng.n_substeps + eng.n_substeps * n_plume_sub) + r["n_on"] * 3
     out = {"metric": METRIC, "value": round(value, 3), "unit": "epochs/s", "n_gpus": world, "steps": K,
            "warmup": args.warmup, "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32 (FP64 ledgers)", "data": "synthetic (seeded, reference config shapes)",
